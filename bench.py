@@ -1,0 +1,444 @@
+"""Benchmark of the B200 cell-grid Lennard-Jones path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2]
+
+A step is one pass of the hot path over one synthetic system: the cell-grid
+build (count, scan, scatter, within-cell sort) and the truncated-LJ pair
+kernel (energy, force, totals).  Default workload: 10,000,000 particles
+uniform in [0,1)^3 from the seeded drand48 generator, cutoff 0.01, cell
+width = cutoff (100^3 cells), eps = 1, sigma = cutoff / 2.5.
+
+value  = interacting ordered pairs per second over all ranks (inputs resident
+         in HBM; L2 flushed between steps, flush excluded from the timing).
+e2e    = the same metric through lj_simulate_host() with host buffers:
+         positions host->device, step, energy/force/index device->host.
+roofline: the pair kernel, algorithmic flops 8 per candidate pair of the
+         reference's 27-cell stencil + 18 per interacting pair, against the
+         FP32 CUDA-core peak 148 SMs x 128 lanes x 2 flop x the SM clock
+         sampled during the timed region.
+--impl reference times the CPU restatement of the reference's cell-grid
+loop (the reference has no CPU path of its own) on the host cores.
+
+Under torchrun each rank runs its own independent system (seed + rank):
+replicas, weak scaling, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "particle-interaction-with-optix_b200"))
+
+METRIC = "LJ pairs/sec @10M particles, plain vs mixed-precision/batched at ≤1e-5 err"
+FLOP_CANDIDATE = 8
+FLOP_INTERACTING = 18
+
+CONFIGS = {
+    "c1": dict(workload="uniform 100k, rc=0.05", n=100_000, dist="uniform", lo=(0, 0, 0), hi=(1, 1, 1), rc=0.05),
+    "c2": dict(workload="uniform 10M, rc=0.01", n=10_000_000, dist="uniform", lo=(0, 0, 0), hi=(1, 1, 1), rc=0.01),
+    "c3": dict(workload="sphere-shell 4M, rc=0.005", n=4_000_000, dist="sphere", lo=(-0.5,) * 3, hi=(1.5,) * 3,
+               rc=0.005),
+    "c4": dict(workload="uniform 10M, rc=0.02", n=10_000_000, dist="uniform", lo=(0, 0, 0), hi=(1, 1, 1), rc=0.02),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- dist
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(backend):
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    ws, rank, _ = dist_env()
+    if ws > 1 and not dist.is_initialized():
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    return ws, rank
+
+
+def allreduce_max(v: float, ws: int, device=None) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(v: float, ws: int, device=None) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- cpu baseline
+class CpuBaseline:
+    """The oracle's restatement of the reference's cell-grid loop (27-cell
+    stencil per particle, config law, FP32) on the host cores.  Set-up
+    generates and bins the whole system once (timed, one thread); each step
+    runs the pair loop over the first targets in cell order, sized to a time
+    budget, and charges the binning time per target."""
+
+    def __init__(self, cfg, seed):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ljoracle as O
+
+        self.O = O
+        n = cfg["n"]
+        if cfg["dist"] == "uniform":
+            x, y, z = O.generate_uniform(seed, n, cfg["lo"], cfg["hi"])
+        else:
+            x, y, z = O.generate_sphere(seed, n, (0.5, 0.5, 0.5), 1.0)
+        self.g = O.grid_from_box(cfg["lo"], cfg["hi"], cfg["rc"])
+        t0 = time.perf_counter()
+        self.b = O.bin_particles(self.g, x, y, z, O.ORDER_INDEX)
+        self.t_bin = time.perf_counter() - t0
+        self.n, self.rc = n, cfg["rc"]
+        self.sigma = float(np.float32(self.rc) / np.float32(2.5))
+        self.e = np.empty(n, np.float32)
+        self.f = np.empty((n, 3), np.float32)
+        self.threads = O.max_threads()
+        self.k1 = min(n, 20_000)
+
+    def step(self, budget_s):
+        while True:
+            t0 = time.perf_counter()
+            pairs = self.O.config_forces_f32_range(self.g, self.b, 0, self.k1, self.rc, 1.0, self.sigma, self.e,
+                                                   self.f, self.threads)
+            dt = time.perf_counter() - t0
+            if dt > budget_s / 3 or self.k1 == self.n:
+                break
+            self.k1 = min(self.n, int(self.k1 * min(8.0, max(1.5, budget_s / max(dt, 1e-4)))))
+        t_step = dt + self.t_bin * (self.k1 / self.n)
+        self.last = {"value": pairs / t_step, "unit": "pairs/s", "cores": self.threads, "kind": "port",
+                     "sample": f"binning of all {self.n} particles once ({self.t_bin:.2f}s, 1 thread, charged per "
+                               f"target) + pair loop over the first {self.k1} sorted targets ({pairs} pairs, "
+                               f"{dt:.2f}s, {self.threads} threads)"}
+        return self.last
+
+
+def run_reference(args, cfg):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    cb = CpuBaseline(cfg, args.seed)
+    per_step = max(0.3, min(4.0, 150.0 / max(1, args.steps + args.warmup)))
+    for _ in range(max(args.warmup, 0)):
+        cb.step(per_step)
+    vals = [cb.step(per_step)["value"] for _ in range(args.steps)]
+    value = float(np.median(vals))
+    info = cb.last
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded drand48)",
+            "config": {"workload": cfg["workload"], "n": cfg["n"], "cutoff": cfg["rc"], "path": "cpu cell-grid loop"},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": info["cores"], "kind": "port",
+                             "sample": info["sample"]},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- ours
+def run_ours(args, cfg):
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+    init_dist("nccl" if ws > 1 else "gloo")
+    import ljcell
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    ctx = ljcell.Context(dev.index, stream)
+    seed = args.seed + rank
+    n, rc = cfg["n"], cfg["rc"]
+    g = ljcell.grid_from_box(cfg["lo"], cfg["hi"], rc)
+    p = ljcell.params(rc)
+    if cfg["dist"] == "uniform":
+        soa, _ = ctx.generate_uniform(seed, n, cfg["lo"], cfg["hi"])
+    else:
+        soa, _ = ctx.generate_sphere(seed, n, (0.5, 0.5, 0.5), 1.0)
+    x, y, z = soa["x"], soa["y"], soa["z"]
+    b = ctx.alloc_binned(g, n, ljcell.ORDER_X)
+    energy, force, tot = ctx.alloc_outputs(n)
+    cand = torch.zeros(1, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def step():
+        ctx.bin(g, x, y, z, order=ljcell.ORDER_X, out=b)
+        ctx.compute(g, p, b, energy, force, tot)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ctx.sync()
+    ctx.count_candidates(g, b.offsets, cand)
+    ctx.sync()
+    c_ref = int(cand.item())
+    pairs = ljcell.totals_from_tensor(tot)["pairs"]
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        for k in range(K):
+            flush.fill_(k & 0xFF)                      # L2 flush, outside the timed events
+            ev[k][0].record(stream)
+            ctx.bin(g, x, y, z, order=ljcell.ORDER_X, out=b)
+            ev[k][1].record(stream)
+            ctx.compute(g, p, b, energy, force, tot)
+            ev[k][2].record(stream)
+        torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    ctx.sync()
+    t_bin = np.array([ev[k][0].elapsed_time(ev[k][1]) for k in range(K)])
+    t_pair = np.array([ev[k][1].elapsed_time(ev[k][2]) for k in range(K)])
+    t_step_ms = float((t_bin + t_pair).sum()) / K
+    t_max_ms = allreduce_max(t_step_ms, ws, dev)
+    total_pairs = allreduce_sum(float(pairs), ws, dev)
+    value = total_pairs / (t_max_ms * 1e-3)
+
+    clocks = clk.summary()
+    sm_mhz = clocks["sm_mhz"] or 1965.0
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_tflops = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+    algo_flops = FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs
+    pair_ms = float(t_pair.mean())
+    achieved = algo_flops / (pair_ms * 1e-3) / 1e12
+    traffic = read_traffic("k_pair_config", cfg["workload"])
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(ctx, g, p, x, y, z, n, K, ws, dev, total_pairs, pairs)
+
+    ref_gpu = None
+
+    if rank == 0 and ws == 1 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu(cfg, x, y, z, ctx, g)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cb = CpuBaseline(cfg, args.seed)
+        cb.step(2.0)
+        c = cb.step(12.0)
+        cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": K, "warmup": args.warmup,
+            "ms_per_step": t_max_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded drand48, device generated)",
+            "config": {"workload": cfg["workload"], "n_per_gpu": n, "cutoff": rc, "sigma": p.sigma,
+                       "cells": g.ncells, "order": "x-sorted within cells", "mode": "plain fp32",
+                       "l2": "flushed between steps (256 MiB write), flush excluded from timing",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single gpu"},
+            "stage_ms": {"bin": float(t_bin.mean()), "pair": pair_ms},
+            "pairs_per_step": pairs, "candidate_pairs_per_step": c_ref,
+            "candidate_pairs_per_s": c_ref * ws / (t_max_ms * 1e-3),
+            "particles_per_s": n * ws / (t_max_ms * 1e-3),
+            "roofline": {"kernel": "k_pair_config", "bound": "fp32", "achieved": achieved, "peak": peak_tflops,
+                         "unit": "TFLOP/s", "frac": achieved / peak_tflops, "traffic": traffic,
+                         "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 flop x {sm_mhz:.0f} MHz (median sampled "
+                                        "SM clock; MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
+                         "algorithmic_flops": algo_flops},
+            "e2e": e2e,
+            "gpu_launches": 6 * K,
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        if ref_gpu:
+            line["reference_gpu"] = ref_gpu
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_e2e(ctx, g, p, x, y, z, n, K, ws, dev, total_pairs, pairs):
+    """Same metric through lj_simulate_host(): pinned host positions in,
+    energy / force / index out, copies inside the timed region."""
+    import torch
+
+    hx, hy, hz = (torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(3))
+    hx.copy_(x)
+    hy.copy_(y)
+    hz.copy_(z)
+    he = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    hf = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    hidx = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    hxn, hyn, hzn, hen, hfn, hin = (t.numpy() for t in (hx, hy, hz, he, hf, hidx))
+    for _ in range(2):
+        ctx.simulate_host(g, p, hxn, hyn, hzn, hen, hfn, hin)
+    steps = max(3, min(K, 20))
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        tt = ctx.simulate_host(g, p, hxn, hyn, hzn, hen, hfn, hin)
+    e2e_s = allreduce_max((time.perf_counter() - t0) / steps, ws, dev)
+    if tt.pairs != pairs:
+        raise RuntimeError(f"end-to-end pair count {tt.pairs} differs from the device path {pairs}")
+    return {"value": total_pairs / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": 12 * n,
+            "d2h_bytes_per_step": 20 * n + 32, "ms_per_step": e2e_s * 1e3, "steps": steps}
+
+
+def read_traffic(kernel, workload):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for ln in open(path):
+        parts = [s.strip() for s in ln.split("|")]
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+def reference_gpu(cfg, x, y, z, ctx, g):
+    """The reference's own kernels (cudaLJ.cu, built from source) on the same
+    positions, reference law and stencil: candidate pairs/s of its pair kernel
+    and its binning time.  Needs oracle/_ref/libljref.so."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ljoracle as O
+
+    if not O.ref_available() or cfg["dist"] != "uniform" or tuple(cfg["lo"]) != (0, 0, 0):
+        return None
+    box = float(cfg["hi"][0])
+    below = np.nextafter(np.float32(box), np.float32(0))
+    hx, hy, hz = (np.minimum(t.detach().cpu().numpy(), below).astype(np.float32) for t in (x, y, z))
+    r = O.ref_run(hx, hy, hz, box, cfg["rc"], reps=3)
+    ms = r.stage_ms
+    # our compat kernel on the same positions, for a like-for-like pair-kernel time
+    import torch
+    import ljcell
+
+    gc = ljcell.grid_compat(box, cfg["rc"])
+    d = [torch.from_numpy(a).cuda() for a in (hx, hy, hz)]
+    b = ctx.bin(gc, *d, order=ljcell.ORDER_INDEX)
+    v = ctx.compute_compat(gc, b)
+    ctx.sync()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(3):
+        s.record()
+        ctx.compute_compat(gc, b, v)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    return {"what": "reference cudaLJ.cu kernels built from source for sm_100a, same positions, reference law",
+            "candidate_pairs": r.nbinter, "pair_kernel_ms": float(ms[5]), "binning_ms": float(ms[6]),
+            "scan_ms": float(ms[1]), "candidate_pairs_per_s": r.nbinter / (float(ms[5]) * 1e-3),
+            "ours_compat_pair_kernel_ms": best, "ours_compat_candidate_pairs_per_s": r.nbinter / (best * 1e-3)}
+
+
+def main():
+    args = parse()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        return run_reference(args, cfg)
+    return run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,212 @@
+/*
+ * ljcell.h -- C ABI of the B200 cell-grid Lennard-Jones path.
+ *
+ * Drop-in boundary for the cell-grid path of OptixLJ (Cuda-version/cudaLJ.cu).
+ * The reference has no library API: its de facto interface is the set of
+ * stage kernels called by executeSimulation() (cudaLJ.cu:515-677) on a
+ * ParticlesContainer<float> (cudaLJ.cu:60-67) and CellDescriptor array
+ * (cudaLJ.cu:91-94).  Each entry point below replaces one of those stages and
+ * cites it.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Pointers documented as "device" are CUDA
+ *    device pointers; "host" pointers are ordinary memory.
+ *  - Every call that launches work is asynchronous on the context's stream
+ *    (lj_set_stream; 0 = legacy default stream).  Scalar results are written to
+ *    device memory; lj_sync() waits and reports errors that kernels recorded
+ *    in the context's device status word (LJ_ERANGE for non-finite positions,
+ *    LJ_ETIMEOUT for a bounded wait that gave up).
+ *  - Errors are returned, never exit(): the reference's CUDA_ASSERT called
+ *    exit(1) (cudaLJ.cu:17-26).
+ *  - One context per host thread; contexts are not shared between threads.
+ *  - The context owns its scratch memory (scan tile states, tickets, reduction
+ *    partials) and reuses it across calls; the caller owns every buffer it
+ *    passes in.
+ */
+#ifndef LJCELL_H
+#define LJCELL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LJCELL_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LJ_API __attribute__((visibility("default")))
+#else
+#define LJ_API
+#endif
+
+typedef enum {
+    LJ_OK = 0,
+    LJ_EINVAL = 1,       /* bad argument (NULL pointer, size, cutoff <= 0, ...) */
+    LJ_ENOMEM = 2,       /* device allocation of context scratch failed */
+    LJ_ECUDA = 3,        /* a CUDA runtime call failed */
+    LJ_ETIMEOUT = 4,     /* a bounded device-side wait gave up */
+    LJ_ERANGE = 5,       /* non-finite particle coordinate seen by the binning */
+    LJ_EUNSUPPORTED = 6  /* size or mode outside what this build supports */
+} lj_status;
+
+/* Within-cell order of the sorted particles.  The reference's order comes
+ * from atomic tickets (cudaLJ.cu:462) and changes run to run; both orders
+ * here are deterministic functions of the input. */
+typedef enum {
+    LJ_ORDER_INDEX = 0, /* ascending original index: a stable scatter on the cell key */
+    LJ_ORDER_X = 1      /* ascending x, ties by original index (enables x-windowed pair search) */
+} lj_order;
+
+typedef struct lj_ctx lj_ctx;
+
+/* == ParticlesContainer<float> (cudaLJ.cu:60-67): device SoA arrays. */
+typedef struct {
+    float* x;
+    float* y;
+    float* z;
+    float* v;
+    int* index;
+    int nbParticles;
+} lj_particles;
+
+/* == CellDescriptor (cudaLJ.cu:91-94). */
+typedef struct {
+    int nbParticleInCell;
+    int offsetInContainer;
+} lj_cell_desc;
+
+/* Regular cell grid: cell (cx,cy,cz) covers origin + [c, c+1) * width per
+ * axis; linear index (cz * dim[1] + cy) * dim[0] + cx as CellCoordToIndex
+ * (cudaLJ.cu:128-134).  The reference fixes origin = 0 (cudaLJ.cu:525). */
+typedef struct {
+    float origin[3];
+    float width;
+    int dim[3];
+} lj_grid;
+
+/* Truncated LJ parameters: V = 4 eps [(sigma/r)^12 - (sigma/r)^6], r < cutoff. */
+typedef struct {
+    float cutoff;
+    float epsilon;
+    float sigma;
+} lj_params;
+
+/* Global results of a compute call (device or host memory as documented). */
+typedef struct {
+    double energy;            /* E = 1/2 sum_i e_i */
+    double virial;            /* W = sum_{i<j} r_ij . F_ij */
+    unsigned long long pairs; /* interacting ordered pairs (i != j, r < cutoff) */
+    unsigned long long pad;
+} lj_totals;
+
+/* ------------------------------------------------------------------ context */
+LJ_API int lj_abi_version(void);
+LJ_API const char* lj_status_str(lj_status s);
+
+/* Creates a context on `device` issuing work on `stream` (a cudaStream_t,
+ * NULL = legacy default stream). */
+LJ_API lj_status lj_create(lj_ctx** out, int device, void* stream);
+LJ_API lj_status lj_destroy(lj_ctx* ctx);
+LJ_API lj_status lj_set_stream(lj_ctx* ctx, void* stream);
+/* Waits for the context's stream, then returns (and clears) the first error
+ * recorded by its kernels. */
+LJ_API lj_status lj_sync(lj_ctx* ctx);
+
+/* --------------------------------------------------------------- generation
+ * Replaces InitRandStates + InitParticles / InitParticlesSphere
+ * (cudaLJ.cu:98-105, 174-220).  The generator is the POSIX drand48 LCG with
+ * srand48(seed) semantics, drawn in the order of the reference's host
+ * generator (SDK/optixMultiSphere/optixSphere.cpp:132-155), evaluated on the
+ * device by jump-ahead.  Outputs: SoA x, y, z (device), index[i] = i and
+ * v[i] = -1 as InitParticles does (each of x/y/z/index/v may be NULL), and
+ * optionally an AoS point3d array xyz[3n] (device, may be NULL). */
+LJ_API lj_status lj_generate_uniform(lj_ctx* ctx, uint64_t seed, int n, const float lo[3], const float hi[3],
+                              lj_particles* out, float* xyz);
+LJ_API lj_status lj_generate_sphere(lj_ctx* ctx, uint64_t seed, int n, const float centre[3], float radius,
+                             lj_particles* out, float* xyz);
+
+/* ------------------------------------------------------------------- grid
+ * Host-only.  dim = int(extent / cutoff) in float, at least 1, as
+ * executeSimulation computes GridDim (cudaLJ.cu:528-530). */
+LJ_API lj_status lj_grid_from_box(const float lo[3], const float hi[3], float cutoff, lj_grid* out);
+/* The reference's grid: origin 0, box [0, box_width)^3 (cudaLJ.cu:525-530). */
+LJ_API lj_status lj_grid_compat(float box_width, float cutoff, lj_grid* out);
+
+/* ----------------------------------------------------------------- binning */
+/* Per-cell counts, replaces ComputeNbParticlePerCells (cudaLJ.cu:345-383).
+ * Positions are read as x[i*stride], y[i*stride], z[i*stride] (stride 1 for
+ * SoA, 3 for an AoS point3d array with y = x + 1, z = x + 2).  counts[ncells]
+ * (device) is overwritten. */
+LJ_API lj_status lj_count_cells(lj_ctx* ctx, const lj_grid* g, int n, const float* x, const float* y, const float* z,
+                         int stride, int* counts);
+
+/* Exclusive scan offsets[0..ncells] (offsets[0] = 0, offsets[ncells] = total),
+ * replaces PrefixFullV2 (prefixsum.hpp:160-215) as called at cudaLJ.cu:621-622
+ * (memset prefix, scan into prefix + 1).  Single pass, decoupled look-back,
+ * no per-call allocation, no host synchronisation.  Device pointers. */
+LJ_API lj_status lj_exclusive_scan(lj_ctx* ctx, const int* counts, long long ncells, int* offsets);
+
+/* Cell descriptors from offsets, replaces InitNewCells (cudaLJ.cu:428-439). */
+LJ_API lj_status lj_cell_descriptors(lj_ctx* ctx, const int* offsets, long long ncells, lj_cell_desc* cells);
+
+/* The whole cell-grid build, replaces the binning sequence of
+ * executeSimulation (cudaLJ.cu:614-634): count, scan, descriptors and the
+ * scatter of MoveParticlesToNewCells (cudaLJ.cu:441-471), made deterministic
+ * (`order`).  Device pointers:
+ *   in            positions as for lj_count_cells (stride 1 or 3)
+ *   counts        [ncells]        per-cell occupancy                (required)
+ *   offsets       [ncells + 1]    exclusive prefix of counts        (required)
+ *   cells         [ncells]        CellDescriptor view               (may be NULL)
+ *   sorted        SoA x, y, z, index of the particles in cell order  (may be NULL;
+ *                 any member may be NULL; v is not touched, as in the reference)
+ *   sorted_xyzi   [4n] float4 per particle: x, y, z, original index bit-cast
+ *                 to float; 16-byte aligned                        (required)
+ *   sorted_cell   [n] cell id per sorted particle                   (required) */
+LJ_API lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x, const float* y, const float* z, int stride,
+                 lj_order order, int* counts, int* offsets, lj_cell_desc* cells, lj_particles* sorted,
+                 float* sorted_xyzi, int* sorted_cell);
+
+/* ----------------------------------------------------------- interactions */
+/* Candidate ordered pairs of the clamped 27-cell stencil, no distance test:
+ * replaces ComputeNbInteractions (cudaLJ.cu:255-297).  *d_count (device) is
+ * overwritten. */
+LJ_API lj_status lj_count_candidates(lj_ctx* ctx, const lj_grid* g, const int* offsets, unsigned long long* d_count);
+
+/* Reference pair law ("compat"): per-particle energy v[k] of sorted particle
+ * k, summed over every particle of the clamped 27-cell stencil except itself,
+ * with 4 eps ((s/r)^12 - (s/r)^6), eps = s = 1, r = sqrt(d.d + 1e-5) and no
+ * cutoff test: replaces ComputeParticleInterationsParPartNoLoop
+ * (cudaLJ.cu:299-341).  Device pointers from lj_bin. */
+LJ_API lj_status lj_compute_compat(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi, const int* sorted_cell,
+                            const int* offsets, float* v);
+
+/* Truncated LJ with forces (the configuration law; not in the reference):
+ * for i != j and r < cutoff, e_k = 4 eps sum (s^12 - s^6) and
+ * F_k = 24 eps sum r^-2 (2 s^12 - s^6) (p_k - p_j), s = sigma / r, built from
+ * r^-2.  The distance test is d = p_j - p_k (float), r2 = fmaf(dz, dz,
+ * fmaf(dy, dy, dx * dx)), interacting iff r2 < cutoff * cutoff.  `order` must
+ * be the order the particles were binned with (LJ_ORDER_X enables the
+ * x-windowed search).  Outputs in sorted order (device, each may be NULL):
+ * energy[n], force[3n] (point3d), totals (one lj_totals). */
+LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* sorted_xyzi,
+                     const int* sorted_cell, const int* offsets, lj_order order, float* energy, float* force,
+                     lj_totals* totals);
+
+/* ------------------------------------------------------------- end to end
+ * One call with HOST buffers, the shape of executeSimulation's step
+ * (cudaLJ.cu:613-653) without the generation: copies positions to the device,
+ * bins (LJ_ORDER_X), computes the truncated law and copies back, in sorted
+ * order, energy[n], force[3n] and index[n] (original index of each sorted
+ * particle), plus the totals.  Device buffers are owned by the context and
+ * reused.  Output pointers may be NULL.  Synchronises before returning. */
+LJ_API lj_status lj_simulate_host(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* hx,
+                           const float* hy, const float* hz, float* h_energy, float* h_force, int* h_index,
+                           lj_totals* h_totals);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LJCELL_H */

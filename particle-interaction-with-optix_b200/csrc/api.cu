@@ -1,0 +1,225 @@
+// api.cu -- context, scratch memory, status and the end-to-end entry of the C ABI.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "ljcell_internal.cuh"
+
+namespace ljc {
+
+lj_status grow(void** p, size_t* cap, size_t need) {
+    if (need <= *cap && *p) return LJ_OK;
+    if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+        *cap = 0;
+    }
+    size_t want = need + need / 8 + 256;
+    if (cudaMalloc(p, want) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return LJ_ENOMEM;
+    }
+    *cap = want;
+    return LJ_OK;
+}
+
+lj_status last_launch_status() {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LJ_OK : LJ_ECUDA;
+}
+
+// Switches to the context's device for the duration of one API call.
+struct DeviceScope {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceScope(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            ok = false;
+            return;
+        }
+        if (prev != dev && cudaSetDevice(dev) != cudaSuccess) ok = false;
+    }
+    ~DeviceScope() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace ljc
+
+using namespace ljc;
+
+extern "C" int lj_abi_version(void) { return LJCELL_ABI_VERSION; }
+
+extern "C" const char* lj_status_str(lj_status s) {
+    switch (s) {
+        case LJ_OK: return "ok";
+        case LJ_EINVAL: return "invalid argument";
+        case LJ_ENOMEM: return "device allocation failed";
+        case LJ_ECUDA: return "CUDA runtime error";
+        case LJ_ETIMEOUT: return "bounded device wait timed out";
+        case LJ_ERANGE: return "non-finite coordinate or out-of-range index";
+        case LJ_EUNSUPPORTED: return "unsupported size or mode";
+    }
+    return "unknown status";
+}
+
+extern "C" lj_status lj_create(lj_ctx** out, int device, void* stream) {
+    if (!out) return LJ_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess) {
+        cudaGetLastError();
+        return LJ_ECUDA;
+    }
+    if (device < 0 || device >= ndev) return LJ_EINVAL;
+    DeviceScope scope(device);
+    if (!scope.ok) return LJ_ECUDA;
+    lj_ctx* c = new (std::nothrow) lj_ctx();
+    if (!c) return LJ_ENOMEM;
+    std::memset(c, 0, sizeof(*c));
+    c->device = device;
+    c->stream = static_cast<cudaStream_t>(stream);
+    if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        delete c;
+        return LJ_ECUDA;
+    }
+    if (cudaMalloc(&c->d_status, 256) != cudaSuccess || cudaMemset(c->d_status, 0, 256) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return LJ_ENOMEM;
+    }
+    c->d_cand = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(c->d_status) + 64);
+    *out = c;
+    return LJ_OK;
+}
+
+extern "C" lj_status lj_destroy(lj_ctx* c) {
+    if (!c) return LJ_EINVAL;
+    DeviceScope scope(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    else cudaDeviceSynchronize();
+    cudaFree(c->d_status);
+    cudaFree(c->scan_state);
+    cudaFree(c->cell_ticket);
+    cudaFree(c->tmp4);
+    cudaFree(c->large_cells);
+    cudaFree(c->red);
+    cudaFree(c->e2e);
+    delete c;
+    return LJ_OK;
+}
+
+extern "C" lj_status lj_set_stream(lj_ctx* c, void* stream) {
+    if (!c) return LJ_EINVAL;
+    c->stream = static_cast<cudaStream_t>(stream);
+    return LJ_OK;
+}
+
+extern "C" lj_status lj_sync(lj_ctx* c) {
+    if (!c) return LJ_EINVAL;
+    DeviceScope scope(c->device);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return LJ_ECUDA;
+    unsigned flags = 0;
+    if (cudaMemcpy(&flags, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) return LJ_ECUDA;
+    if (flags) {
+        if (cudaMemset(c->d_status, 0, sizeof(unsigned)) != cudaSuccess) return LJ_ECUDA;
+        if (flags & kFlagTimeout) return LJ_ETIMEOUT;
+        return LJ_ERANGE;
+    }
+    return LJ_OK;
+}
+
+extern "C" lj_status lj_grid_from_box(const float lo[3], const float hi[3], float cutoff, lj_grid* out) {
+    if (!lo || !hi || !out || !(cutoff > 0.0f)) return LJ_EINVAL;
+    lj_grid g;
+    for (int d = 0; d < 3; ++d) {
+        const float ext = hi[d] - lo[d];
+        if (!(ext > 0.0f)) return LJ_EINVAL;
+        const float q = ext / cutoff;
+        if (!(q < 2147483647.0f)) return LJ_EUNSUPPORTED;
+        const int G = static_cast<int>(q);
+        g.dim[d] = G < 1 ? 1 : G;
+        g.origin[d] = lo[d];
+    }
+    g.width = cutoff;
+    if ((long long)g.dim[0] * g.dim[1] * g.dim[2] > 2147483646LL) return LJ_EUNSUPPORTED;
+    *out = g;
+    return LJ_OK;
+}
+
+extern "C" lj_status lj_grid_compat(float box_width, float cutoff, lj_grid* out) {
+    const float lo[3] = {0.f, 0.f, 0.f};
+    const float hi[3] = {box_width, box_width, box_width};
+    return lj_grid_from_box(lo, hi, cutoff, out);
+}
+
+extern "C" lj_status lj_simulate_host(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx,
+                                      const float* hy, const float* hz, float* h_energy, float* h_force,
+                                      int* h_index, lj_totals* h_totals) {
+    if (!c || !g || !p || n < 0 || (n > 0 && (!hx || !hy || !hz))) return LJ_EINVAL;
+    DeviceScope scope(c->device);
+    if (!scope.ok) return LJ_ECUDA;
+    const long long nc = (long long)g->dim[0] * g->dim[1] * g->dim[2];
+    if (nc < 1 || nc > 2147483646LL) return LJ_EINVAL;
+    const size_t N = (size_t)(n > 0 ? n : 1);
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t b_pos = up(3 * N * sizeof(float));
+    const size_t b_cnt = up((size_t)nc * sizeof(int));
+    const size_t b_off = up(((size_t)nc + 1) * sizeof(int));
+    const size_t b_x4 = up(N * 16);
+    const size_t b_cell = up(N * sizeof(int));
+    const size_t b_e = up(N * sizeof(float));
+    const size_t b_f = up(3 * N * sizeof(float));
+    const size_t b_idx = up(N * sizeof(int));
+    const size_t b_tot = up(sizeof(lj_totals));
+    const size_t need = b_pos + b_cnt + b_off + b_x4 + b_cell + b_e + b_f + b_idx + b_tot;
+    lj_status s = grow(&c->e2e, &c->e2e_bytes, need);
+    if (s != LJ_OK) return s;
+    char* base = static_cast<char*>(c->e2e);
+    float* dpos = reinterpret_cast<float*>(base);
+    base += b_pos;
+    int* dcnt = reinterpret_cast<int*>(base);
+    base += b_cnt;
+    int* doff = reinterpret_cast<int*>(base);
+    base += b_off;
+    float* dx4 = reinterpret_cast<float*>(base);
+    base += b_x4;
+    int* dcell = reinterpret_cast<int*>(base);
+    base += b_cell;
+    float* de = reinterpret_cast<float*>(base);
+    base += b_e;
+    float* df = reinterpret_cast<float*>(base);
+    base += b_f;
+    int* didx = reinterpret_cast<int*>(base);
+    base += b_idx;
+    lj_totals* dtot = reinterpret_cast<lj_totals*>(base);
+    cudaStream_t st = c->stream;
+    const size_t pb = (size_t)n * sizeof(float);
+    if (n > 0) {
+        if (cudaMemcpyAsync(dpos, hx, pb, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(dpos + N, hy, pb, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(dpos + 2 * N, hz, pb, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return LJ_ECUDA;
+    }
+    lj_particles sorted{};
+    sorted.index = didx;
+    s = lj_bin(c, g, n, dpos, dpos + N, dpos + 2 * N, 1, LJ_ORDER_X, dcnt, doff, nullptr, &sorted, dx4, dcell);
+    if (s != LJ_OK) return s;
+    s = lj_compute(c, g, p, n, dx4, dcell, doff, LJ_ORDER_X, h_energy ? de : nullptr, h_force ? df : nullptr, dtot);
+    if (s != LJ_OK) return s;
+    if (n > 0) {
+        if (h_energy && cudaMemcpyAsync(h_energy, de, pb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return LJ_ECUDA;
+        if (h_force && cudaMemcpyAsync(h_force, df, 3 * pb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return LJ_ECUDA;
+        if (h_index && cudaMemcpyAsync(h_index, didx, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st) !=
+                           cudaSuccess)
+            return LJ_ECUDA;
+    }
+    if (h_totals && cudaMemcpyAsync(h_totals, dtot, sizeof(lj_totals), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return LJ_ECUDA;
+    return lj_sync(c);
+}

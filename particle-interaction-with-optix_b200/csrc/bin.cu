@@ -1,0 +1,582 @@
+// bin.cu -- the cell-grid build on the device.
+//
+// Replaces the binning sequence of executeSimulation (cudaLJ.cu:614-634):
+//   ComputeNbParticlePerCells (cudaLJ.cu:345-383)  -> k_count   (warp-aggregated
+//        per-cell counting; the same atomic hands out each particle's ticket)
+//   PrefixFullV2 (prefixsum.hpp:160-215)           -> k_scan    (single-pass
+//        decoupled look-back exclusive scan; no recursion, no allocation, no
+//        host synchronisation)
+//   InitNewCells (cudaLJ.cu:428-439)               -> k_descriptors / folded into k_cell_sort
+//   MoveParticlesToNewCells (cudaLJ.cu:441-471)    -> k_scatter + k_cell_sort
+//        (ticket scatter, then a per-cell sort that makes the order a pure
+//        function of the input, repacking positions as float4 x, y, z, index)
+// and ComputeNbInteractions (cudaLJ.cu:255-297) -> k_candidates (per cell
+// instead of per particle).
+#include <climits>
+
+#include "ljcell_internal.cuh"
+
+namespace ljc {
+
+// ---------------------------------------------------------------- counting
+// One thread per particle, grid-stride by whole warps.  Lanes that share a
+// cell elect a leader (__match_any_sync) which adds the group's size with one
+// atomic; each lane's ticket is the leader's old value plus its rank in the
+// group.  Tickets give a slot inside the cell; their order is not
+// deterministic, which k_cell_sort fixes.
+template <bool TICKETS>
+__global__ void __launch_bounds__(256) k_count(GridDev g, const float* __restrict__ x, const float* __restrict__ y,
+                                               const float* __restrict__ z, int stride, int n,
+                                               int* __restrict__ counts, int2* __restrict__ ct,
+                                               unsigned* status) {
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = gwarp * 32; base < n; base += nwarps * 32) {
+        const long long i = base + lane;
+        const bool valid = i < n;
+        int cell = -1 - lane;  // distinct key for inactive lanes
+        if (valid) {
+            const float px = x[i * stride], py = y[i * stride], pz = z[i * stride];
+            if (!(isfinite(px) && isfinite(py) && isfinite(pz))) atomicOr(status, kFlagNonFinite);
+            cell = cell_of(g, px, py, pz);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, cell);
+        const int leader = __ffs(peers) - 1;
+        int first = 0;
+        if (valid && lane == leader) first = atomicAdd(&counts[cell], __popc(peers));
+        first = __shfl_sync(0xffffffffu, first, leader);
+        if (TICKETS && valid) ct[i] = make_int2(cell, first + __popc(peers & lanemask_lt()));
+    }
+}
+
+// ---------------------------------------------------------------- scan
+// Exclusive scan of int counts[n] into offsets[0..n] (offsets[n] = total).
+// Tiles of 4096 items (256 threads x 16), tile index taken from an atomic
+// counter so every predecessor tile is already running.  Each warp scans 512
+// items in a striped layout (coalesced int4 loads and stores); warp 0 then
+// publishes the tile aggregate and looks back over predecessors, 32 tiles at a
+// time, until it meets an inclusive prefix.  Tile state = 2-bit flag | 62-bit
+// value in one 64-bit word, so flag and value become visible together.  The
+// look-back wait is bounded: on timeout it records kFlagTimeout and goes on.
+constexpr int kScanThreads = 256;
+constexpr int kScanTile = 4096;
+constexpr unsigned long long kStAgg = 1ULL << 62;
+constexpr unsigned long long kStPre = 2ULL << 62;
+constexpr unsigned long long kStVal = (1ULL << 62) - 1ULL;
+constexpr unsigned kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned long long ld_state(const unsigned long long* p) {
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+__device__ __forceinline__ void st_state(unsigned long long* p, unsigned long long v) {
+    *reinterpret_cast<volatile unsigned long long*>(p) = v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan(const int* __restrict__ counts, int* __restrict__ offsets,
+                                                       long long n, long long ntiles,
+                                                       unsigned long long* tile_state, unsigned* tile_counter,
+                                                       int vec_ok, unsigned* status) {
+    __shared__ unsigned s_tile;
+    __shared__ long long s_warp[8];
+    __shared__ long long s_prefix;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= ntiles) return;  // defensive: more CTAs than tiles
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long tbase = tile * kScanTile;
+    const long long wbase = tbase + warp * 512;
+    const bool full = vec_ok && (tbase + kScanTile <= n);
+    int v[4][4];
+    if (full) {
+#pragma unroll
+        for (int it = 0; it < 4; ++it) {
+            const int4 q = __ldg(reinterpret_cast<const int4*>(counts + wbase + it * 128 + lane * 4));
+            v[it][0] = q.x;
+            v[it][1] = q.y;
+            v[it][2] = q.z;
+            v[it][3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int it = 0; it < 4; ++it)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const long long idx = wbase + it * 128 + lane * 4 + e;
+                v[it][e] = idx < n ? counts[idx] : 0;
+            }
+    }
+    // warp-local exclusive prefixes (sums stay below 2^31: they are particle counts)
+    int carry = 0;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+        const int a0 = v[it][0], a1 = a0 + v[it][1], a2 = a1 + v[it][2], a3 = a2 + v[it][3];
+        int inc = a3;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        const int ex = carry + inc - a3;
+        v[it][0] = ex;
+        v[it][1] = ex + a0;
+        v[it][2] = ex + a1;
+        v[it][3] = ex + a2;
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0) s_warp[warp] = carry;
+    __syncthreads();
+    if (warp == 0) {
+        const long long wt = lane < 8 ? s_warp[lane] : 0;
+        long long inc = wt;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const long long t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        const long long agg = __shfl_sync(0xffffffffu, inc, 7);
+        __syncwarp();
+        if (lane < 8) s_warp[lane] = inc - wt;
+        long long prefix = 0;
+        if (tile == 0) {
+            if (lane == 0) st_state(&tile_state[0], kStPre | (unsigned long long)agg);
+        } else {
+            if (lane == 0) st_state(&tile_state[tile], kStAgg | (unsigned long long)agg);
+            long long pred = tile - 1;
+            unsigned spins = 0;
+            while (true) {
+                const long long t = pred - lane;
+                unsigned long long st = kStPre;  // before tile 0: an inclusive prefix of 0
+                bool gave_up = false;
+                if (t >= 0) {
+                    st = ld_state(&tile_state[t]);
+                    while ((st >> 62) == 0ULL) {
+                        if (++spins > kSpinLimit) {
+                            gave_up = true;
+                            break;
+                        }
+                        __nanosleep(32);
+                        st = ld_state(&tile_state[t]);
+                    }
+                }
+                if (__any_sync(0xffffffffu, gave_up)) {
+                    if (lane == 0) atomicOr(status, kFlagTimeout);
+                    break;
+                }
+                const unsigned pre = __ballot_sync(0xffffffffu, (st >> 62) == 2ULL);
+                if (pre) {
+                    const int first = __ffs(pre) - 1;
+                    const unsigned long long val = lane <= first ? (st & kStVal) : 0ULL;
+                    prefix += (long long)warp_sum(val);
+                    break;
+                }
+                prefix += (long long)warp_sum(st & kStVal);
+                pred -= 32;
+            }
+            if (lane == 0) st_state(&tile_state[tile], kStPre | (unsigned long long)(prefix + agg));
+        }
+        if (lane == 0) {
+            s_prefix = prefix;
+            if (tile == ntiles - 1) offsets[n] = (int)(prefix + agg);
+        }
+    }
+    __syncthreads();
+    const int tp = (int)(s_prefix + s_warp[warp]);
+    if (full) {
+#pragma unroll
+        for (int it = 0; it < 4; ++it)
+            *reinterpret_cast<int4*>(offsets + wbase + it * 128 + lane * 4) =
+                make_int4(tp + v[it][0], tp + v[it][1], tp + v[it][2], tp + v[it][3]);
+    } else {
+#pragma unroll
+        for (int it = 0; it < 4; ++it)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const long long idx = wbase + it * 128 + lane * 4 + e;
+                if (idx < n) offsets[idx] = tp + v[it][e];
+            }
+    }
+}
+
+// ---------------------------------------------------------------- scatter
+// Moves each particle to offsets[cell] + ticket as float4 (x, y, z, index
+// bits).  The slot is range-checked so that a corrupted offsets array cannot
+// write out of bounds.
+__global__ void __launch_bounds__(256) k_scatter(const float* __restrict__ x, const float* __restrict__ y,
+                                                 const float* __restrict__ z, int stride, int n,
+                                                 const int2* __restrict__ ct, const int* __restrict__ offsets,
+                                                 float4* __restrict__ tmp, unsigned* status) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int2 c = ct[i];
+        const long long slot = (long long)__ldg(&offsets[c.x]) + c.y;
+        if (slot >= 0 && slot < n)
+            tmp[slot] = make_float4(x[i * stride], y[i * stride], z[i * stride], __int_as_float((int)i));
+        else
+            atomicOr(status, kFlagRange);
+    }
+}
+
+// ---------------------------------------------------------------- within-cell sort
+// Keys: LJ_ORDER_INDEX sorts by original index; LJ_ORDER_X by x, then index.
+// Indices are unique, so keys are unique and the result is a pure function of
+// the input.
+template <int ORDER>
+__device__ __forceinline__ bool key_less(float xa, int ia, float xb, int ib) {
+    if (ORDER == LJ_ORDER_X) return (xa < xb) || (xa == xb && ia < ib);
+    return ia < ib;
+}
+
+struct SortOut {
+    float4* out4;
+    int* out_cell;
+    float* sx;
+    float* sy;
+    float* sz;
+    int* sidx;
+};
+
+__device__ __forceinline__ void emit(const SortOut& o, long long slot, float4 r, int cell) {
+    o.out4[slot] = r;
+    o.out_cell[slot] = cell;
+    if (o.sx) o.sx[slot] = r.x;
+    if (o.sy) o.sy[slot] = r.y;
+    if (o.sz) o.sz[slot] = r.z;
+    if (o.sidx) o.sidx[slot] = __float_as_int(r.w);
+}
+
+constexpr int kWarpSortMax = 2048;
+
+// One warp per group of 32 consecutive cells.  Lanes read the group's offsets
+// (coalesced), write the CellDescriptor view, copy singleton cells directly,
+// and then sort every cell of 2..kWarpSortMax particles cooperatively by
+// ranking (each record's rank = number of smaller keys in its cell).  Larger
+// cells go to a list handled by k_large_sort.
+template <int ORDER>
+__global__ void __launch_bounds__(256) k_cell_sort(const float4* __restrict__ tmp, const int* __restrict__ offsets,
+                                                   long long ncells, int n, SortOut so, lj_cell_desc* cells,
+                                                   int* large, int large_cap, unsigned* status) {
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long g0 = gwarp * 32; g0 < ncells; g0 += nwarps * 32) {
+        const long long c = g0 + lane;
+        const bool in = c < ncells;
+        int o0 = in ? __ldg(&offsets[c]) : 0;
+        const int onext = __shfl_down_sync(0xffffffffu, o0, 1);
+        int o1 = (lane < 31 && c + 1 < ncells) ? onext : (in ? __ldg(&offsets[c + 1]) : 0);
+        o0 = min(max(o0, 0), n);
+        o1 = min(max(o1, o0), n);
+        const int cnt = in ? o1 - o0 : 0;
+        if (cells && in) cells[c] = lj_cell_desc{cnt, o0};
+        if (cnt == 1) emit(so, o0, tmp[o0], (int)c);
+        if (cnt > kWarpSortMax) {
+            const int slot = atomicAdd(&large[0], 1);
+            if (slot < large_cap)
+                large[1 + slot] = (int)c;
+            else
+                atomicOr(status, kFlagRange);
+        }
+        unsigned multi = __ballot_sync(0xffffffffu, cnt > 1 && cnt <= kWarpSortMax);
+        while (multi) {
+            const int src = __ffs(multi) - 1;
+            multi &= multi - 1;
+            const int base = __shfl_sync(0xffffffffu, o0, src);
+            const int m = __shfl_sync(0xffffffffu, cnt, src);
+            const int cell = (int)(g0 + src);
+            if (m <= 32) {
+                const float4 r = lane < m ? tmp[base + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float rx = r.x;
+                const int ri = __float_as_int(r.w);
+                int rank = 0;
+                for (int q = 0; q < m; ++q) {
+                    const float qx = __shfl_sync(0xffffffffu, rx, q);
+                    const int qi = __shfl_sync(0xffffffffu, ri, q);
+                    rank += key_less<ORDER>(qx, qi, rx, ri) ? 1 : 0;
+                }
+                if (lane < m) emit(so, (long long)base + rank, r, cell);
+            } else {
+                for (int b = 0; b < m; b += 32) {
+                    const int e = b + lane;
+                    const bool ok = e < m;
+                    const float4 r = ok ? tmp[base + e] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const int ri = __float_as_int(r.w);
+                    int rank = 0;
+                    for (int q = 0; q < m; ++q) {
+                        const float4 t = tmp[base + q];  // warp-uniform address: one broadcast load
+                        rank += key_less<ORDER>(t.x, __float_as_int(t.w), r.x, ri) ? 1 : 0;
+                    }
+                    if (ok) emit(so, (long long)base + rank, r, cell);
+                }
+            }
+        }
+    }
+}
+
+// Cells larger than kWarpSortMax (rare: clustered or degenerate inputs): one
+// CTA per cell sorts 2048-record chunks in shared memory (bitonic network),
+// then merges runs pairwise, each record finding its place in the partner run
+// by binary search; ping-pong between the cell's tmp and out ranges.
+template <int ORDER>
+__device__ __forceinline__ bool rec_less(const float4& a, const float4& b) {
+    return key_less<ORDER>(a.x, __float_as_int(a.w), b.x, __float_as_int(b.w));
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(1024) k_large_sort(float4* __restrict__ tmp, const int* __restrict__ offsets,
+                                                     int n, SortOut so, const int* __restrict__ large,
+                                                     int large_cap) {
+    __shared__ float4 sbuf[2048];
+    const int count = min(large[0], large_cap);
+    const int tid = threadIdx.x;
+    for (int li = blockIdx.x; li < count; li += gridDim.x) {
+        const int c = large[1 + li];
+        int o = min(max(offsets[c], 0), n);
+        int e1 = min(max(offsets[c + 1], o), n);
+        const int cnt = e1 - o;
+        float4* A = tmp + o;
+        float4* B = so.out4 + o;
+        const float4 sentinel = make_float4(__int_as_float(0x7f800000), 0.f, 0.f, __int_as_float(INT_MAX));
+        for (int ch = 0; ch < cnt; ch += 2048) {
+            const int len = min(2048, cnt - ch);
+            for (int i = tid; i < 2048; i += 1024) sbuf[i] = i < len ? A[ch + i] : sentinel;
+            __syncthreads();
+            for (int k = 2; k <= 2048; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = tid; i < 2048; i += 1024) {
+                        const int p = i ^ j;
+                        if (p > i) {
+                            const bool up = (i & k) == 0;
+                            const float4 a = sbuf[i], b = sbuf[p];
+                            if (rec_less<ORDER>(b, a) == up) {
+                                sbuf[i] = b;
+                                sbuf[p] = a;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            for (int i = tid; i < len; i += 1024) B[ch + i] = sbuf[i];
+            __syncthreads();
+        }
+        float4* src = B;
+        float4* dst = A;
+        for (int width = 2048; width < cnt; width *= 2) {
+            for (int e = tid; e < cnt; e += 1024) {
+                const int run = e / width;
+                const int run_start = run * width;
+                const int pair_start = (run & ~1) * width;
+                const bool left = (run & 1) == 0;
+                const int other = left ? run_start + width : run_start - width;
+                const int other_len = left ? max(0, min(cnt - other, width)) : width;
+                const float4 r = src[e];
+                int lo = 0, hi = other_len;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (rec_less<ORDER>(src[other + mid], r))
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                dst[pair_start + (e - run_start) + lo] = r;
+            }
+            __syncthreads();
+            float4* t = src;
+            src = dst;
+            dst = t;
+        }
+        for (int e = tid; e < cnt; e += 1024) emit(so, (long long)o + e, src[e], c);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- descriptors / candidates
+__global__ void __launch_bounds__(256) k_descriptors(const int* __restrict__ offsets, long long ncells,
+                                                     lj_cell_desc* __restrict__ cells) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int o0 = offsets[c], o1 = offsets[c + 1];
+        cells[c] = lj_cell_desc{o1 - o0, o0};
+    }
+}
+
+// Candidate ordered pairs: sum over cells of count * (stencil occupancy - 1),
+// the stencil being the clamped 3x3x3 block read as 9 rows of consecutive
+// cells.  Integer atomics make the total order-independent.
+__global__ void __launch_bounds__(256) k_candidates(GridDev g, const int* __restrict__ offsets, long long ncells,
+                                                    unsigned long long* out) {
+    __shared__ unsigned long long s[8];
+    unsigned long long acc = 0;
+    const long long gxy = (long long)g.gx * g.gy;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+         c += (long long)gridDim.x * blockDim.x) {
+        const long long cnt = (long long)__ldg(&offsets[c + 1]) - __ldg(&offsets[c]);
+        if (cnt <= 0) continue;
+        const int cz = (int)(c / gxy);
+        const long long r = c - cz * gxy;
+        const int cy = (int)(r / g.gx);
+        const int cx = (int)(r - (long long)cy * g.gx);
+        const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
+        long long s_occ = 0;
+        for (int z = max(cz - 1, 0); z <= min(cz + 1, g.gz - 1); ++z)
+            for (int y = max(cy - 1, 0); y <= min(cy + 1, g.gy - 1); ++y) {
+                const long long rb = ((long long)z * g.gy + y) * g.gx;
+                s_occ += (long long)__ldg(&offsets[rb + xh + 1]) - __ldg(&offsets[rb + xl]);
+            }
+        acc += (unsigned long long)(cnt * (s_occ - 1));
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned long long t = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0ULL;
+        t = warp_sum(t);
+        if (threadIdx.x == 0 && t) atomicAdd(out, t);
+    }
+}
+
+// ---------------------------------------------------------------- host side
+static inline int grid_for(const lj_ctx* ctx, long long items, int per_block, int waves = 8) {
+    long long b = (items + per_block - 1) / per_block;
+    const long long cap = (long long)ctx->sm_count * waves;
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+static lj_status check_grid(const lj_grid* g, long long* ncells) {
+    if (!g || !(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
+    const long long nc = (long long)g->dim[0] * g->dim[1] * g->dim[2];
+    if (nc > (long long)INT_MAX - 1) return LJ_EUNSUPPORTED;
+    *ncells = nc;
+    return LJ_OK;
+}
+
+lj_status launch_scan(lj_ctx* ctx, const int* counts, long long ncells, int* offsets) {
+    const long long ntiles = (ncells + kScanTile - 1) / kScanTile;
+    const size_t need = 256 + (size_t)(ntiles > 0 ? ntiles : 1) * sizeof(unsigned long long);
+    lj_status s = grow(&ctx->scan_state, &ctx->scan_state_bytes, need);
+    if (s != LJ_OK) return s;
+    if (ncells == 0) {
+        if (cudaMemsetAsync(offsets, 0, sizeof(int), ctx->stream) != cudaSuccess) return LJ_ECUDA;
+        return LJ_OK;
+    }
+    if (cudaMemsetAsync(ctx->scan_state, 0, need, ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    unsigned* counter = reinterpret_cast<unsigned*>(ctx->scan_state);
+    unsigned long long* states = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->scan_state) + 256);
+    const int vec_ok = ((reinterpret_cast<uintptr_t>(counts) | reinterpret_cast<uintptr_t>(offsets)) & 15) == 0;
+    k_scan<<<(unsigned)ntiles, kScanThreads, 0, ctx->stream>>>(counts, offsets, ncells, ntiles, states, counter,
+                                                              vec_ok, ctx->d_status);
+    return last_launch_status();
+}
+
+}  // namespace ljc
+
+using namespace ljc;
+
+extern "C" lj_status lj_count_cells(lj_ctx* ctx, const lj_grid* g, int n, const float* x, const float* y,
+                                    const float* z, int stride, int* counts) {
+    long long nc;
+    if (!ctx || n < 0 || !counts || stride < 1) return LJ_EINVAL;
+    lj_status s = check_grid(g, &nc);
+    if (s != LJ_OK) return s;
+    if (n > 0 && (!x || !y || !z)) return LJ_EINVAL;
+    if (cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    if (n == 0) return LJ_OK;
+    k_count<false><<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(to_dev(*g), x, y, z, stride, n, counts, nullptr,
+                                                                  ctx->d_status);
+    return last_launch_status();
+}
+
+extern "C" lj_status lj_exclusive_scan(lj_ctx* ctx, const int* counts, long long ncells, int* offsets) {
+    if (!ctx || ncells < 0 || !offsets || (ncells > 0 && !counts)) return LJ_EINVAL;
+    if (ncells > (long long)INT_MAX - 1) return LJ_EUNSUPPORTED;
+    return launch_scan(ctx, counts, ncells, offsets);
+}
+
+extern "C" lj_status lj_cell_descriptors(lj_ctx* ctx, const int* offsets, long long ncells, lj_cell_desc* cells) {
+    if (!ctx || ncells < 0 || !offsets || !cells) return LJ_EINVAL;
+    if (ncells == 0) return LJ_OK;
+    k_descriptors<<<grid_for(ctx, ncells, 256), 256, 0, ctx->stream>>>(offsets, ncells, cells);
+    return last_launch_status();
+}
+
+extern "C" lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x, const float* y, const float* z,
+                            int stride, lj_order order, int* counts, int* offsets, lj_cell_desc* cells,
+                            lj_particles* sorted, float* sorted_xyzi, int* sorted_cell) {
+    long long nc;
+    if (!ctx || n < 0 || stride < 1 || !counts || !offsets) return LJ_EINVAL;
+    if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
+    lj_status s = check_grid(g, &nc);
+    if (s != LJ_OK) return s;
+    if (n > 0 && (!x || !y || !z || !sorted_xyzi || !sorted_cell)) return LJ_EINVAL;
+    if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
+    const GridDev gd = to_dev(*g);
+    cudaStream_t st = ctx->stream;
+    // scratch: per-particle (cell, ticket) and the unsorted float4 copy
+    const size_t need = (size_t)(n > 0 ? n : 1);
+    if (need > ctx->part_cap) {
+        void* p1 = ctx->cell_ticket;
+        void* p2 = ctx->tmp4;
+        size_t c1 = ctx->part_cap * sizeof(int2), c2 = ctx->part_cap * sizeof(float4);
+        if ((s = grow(&p1, &c1, need * sizeof(int2))) != LJ_OK) return s;
+        ctx->cell_ticket = static_cast<int2*>(p1);
+        if ((s = grow(&p2, &c2, need * sizeof(float4))) != LJ_OK) return s;
+        ctx->tmp4 = static_cast<float4*>(p2);
+        ctx->part_cap = need;
+    }
+    const int large_cap = 4096;
+    if (!ctx->large_cells) {
+        void* p = nullptr;
+        size_t cap = 0;
+        if ((s = grow(&p, &cap, sizeof(int) * (1 + large_cap))) != LJ_OK) return s;
+        ctx->large_cells = static_cast<int*>(p);
+        ctx->large_cap = large_cap;
+    }
+    if (cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, st) != cudaSuccess) return LJ_ECUDA;
+    if (cudaMemsetAsync(ctx->large_cells, 0, sizeof(int), st) != cudaSuccess) return LJ_ECUDA;
+    if (n > 0) {
+        k_count<true><<<grid_for(ctx, n, 256), 256, 0, st>>>(gd, x, y, z, stride, n, counts, ctx->cell_ticket,
+                                                             ctx->d_status);
+        if ((s = last_launch_status()) != LJ_OK) return s;
+    }
+    if ((s = launch_scan(ctx, counts, nc, offsets)) != LJ_OK) return s;
+    if (n > 0) {
+        k_scatter<<<grid_for(ctx, n, 256), 256, 0, st>>>(x, y, z, stride, n, ctx->cell_ticket, offsets, ctx->tmp4,
+                                                         ctx->d_status);
+        if ((s = last_launch_status()) != LJ_OK) return s;
+    }
+    SortOut so{reinterpret_cast<float4*>(sorted_xyzi), sorted_cell, nullptr, nullptr, nullptr, nullptr};
+    if (sorted) {
+        so.sx = sorted->x;
+        so.sy = sorted->y;
+        so.sz = sorted->z;
+        so.sidx = sorted->index;
+    }
+    const int sort_blocks = grid_for(ctx, (nc + 31) / 32, 8, 16);
+    if (order == LJ_ORDER_X) {
+        k_cell_sort<LJ_ORDER_X><<<sort_blocks, 256, 0, st>>>(ctx->tmp4, offsets, nc, n, so, cells, ctx->large_cells,
+                                                            large_cap, ctx->d_status);
+        if ((s = last_launch_status()) != LJ_OK) return s;
+        k_large_sort<LJ_ORDER_X><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so, ctx->large_cells,
+                                                                 large_cap);
+    } else {
+        k_cell_sort<LJ_ORDER_INDEX><<<sort_blocks, 256, 0, st>>>(ctx->tmp4, offsets, nc, n, so, cells,
+                                                                ctx->large_cells, large_cap, ctx->d_status);
+        if ((s = last_launch_status()) != LJ_OK) return s;
+        k_large_sort<LJ_ORDER_INDEX><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so, ctx->large_cells,
+                                                                     large_cap);
+    }
+    return last_launch_status();
+}
+
+extern "C" lj_status lj_count_candidates(lj_ctx* ctx, const lj_grid* g, const int* offsets,
+                                         unsigned long long* d_count) {
+    long long nc;
+    if (!ctx || !offsets || !d_count) return LJ_EINVAL;
+    lj_status s = check_grid(g, &nc);
+    if (s != LJ_OK) return s;
+    if (cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    k_candidates<<<grid_for(ctx, nc, 256), 256, 0, ctx->stream>>>(to_dev(*g), offsets, nc, d_count);
+    return last_launch_status();
+}

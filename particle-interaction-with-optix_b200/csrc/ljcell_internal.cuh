@@ -1,0 +1,108 @@
+// ljcell_internal.cuh -- device-side shared definitions of the B200 cell-grid path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ljcell.h"
+
+namespace ljc {
+
+// Bits of the context's device status word (the kernels OR them in).
+enum : unsigned {
+    kFlagNonFinite = 1u << 0,  // a coordinate was NaN or Inf
+    kFlagTimeout = 1u << 1,    // a bounded spin-wait gave up
+    kFlagRange = 1u << 2,      // an index fell outside its buffer (defensive check)
+};
+
+// Grid passed by value to kernels.
+struct GridDev {
+    float ox, oy, oz, w;
+    int gx, gy, gz;
+};
+
+inline GridDev to_dev(const lj_grid& g) {
+    GridDev d;
+    d.ox = g.origin[0];
+    d.oy = g.origin[1];
+    d.oz = g.origin[2];
+    d.w = g.width;
+    d.gx = g.dim[0];
+    d.gy = g.dim[1];
+    d.gz = g.dim[2];
+    return d;
+}
+
+// Cell coordinate along one axis: int((x - o) / w) with IEEE subtraction and
+// division (PosToCellCoord, cudaLJ.cu:110-119), clamped to [0, g-1]; NaN and
+// negative quotients land in cell 0.
+__device__ __forceinline__ int axis_cell(float x, float o, float w, int g) {
+    const float q = __fdiv_rn(__fsub_rn(x, o), w);
+    if (q >= (float)g) return g - 1;
+    if (q > 0.0f) return __float2int_rz(q);
+    return 0;
+}
+
+__device__ __forceinline__ int cell_of(const GridDev& g, float x, float y, float z) {
+    const int cx = axis_cell(x, g.ox, g.w, g.gx);
+    const int cy = axis_cell(y, g.oy, g.w, g.gy);
+    const int cz = axis_cell(z, g.oz, g.w, g.gz);
+    return (cz * g.gy + cy) * g.gx + cx;
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Approximate reciprocal (PTX rcp.approx.ftz.f32, at most 1 ulp error).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Warp sums.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace ljc
+
+// Opaque context (host side).
+struct lj_ctx {
+    int device;
+    cudaStream_t stream;
+    int sm_count;
+    unsigned* d_status;          // device status word
+    // scratch, grown on demand
+    void* scan_state;            // tile counter + tile status words
+    size_t scan_state_bytes;
+    int2* cell_ticket;           // per particle: cell id, ticket
+    float4* tmp4;                // scatter target before the within-cell sort
+    size_t part_cap;             // capacity (particles) of cell_ticket / tmp4
+    int* large_cells;            // [0] = count, [1..] = ids of cells too large for the warp sort
+    size_t large_cap;
+    void* red;                   // reduction partials + counter
+    size_t red_bytes;
+    unsigned long long* d_cand;  // candidate-count accumulator
+    // end-to-end buffers (lj_simulate_host)
+    void* e2e;
+    size_t e2e_bytes;
+};
+
+namespace ljc {
+// Host helpers shared by the .cu files (defined in api.cu).
+lj_status grow(void** p, size_t* cap, size_t need);
+lj_status last_launch_status();
+}  // namespace ljc

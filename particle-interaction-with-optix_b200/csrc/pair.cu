@@ -1,0 +1,351 @@
+// pair.cu -- the interaction stage on the device.
+//
+// k_pair_compat replaces ComputeParticleInterationsParPartNoLoop
+// (cudaLJ.cu:299-341) with the reference's law and stencil: every particle of
+// the clamped 27-cell block except itself, r = sqrt(d.d + 1e-5), IEEE sqrt and
+// division, 4 eps ((1/r)^12 - (1/r)^6) with eps = sigma = 1, no cutoff.  The 27
+// cells are read as 9 rows of 3 consecutive cells, contiguous in cell order,
+// and positions come as one float4 load instead of three scalar loads.
+//
+// k_pair_config evaluates the truncated law with forces.  One thread per
+// sorted target particle.  For each of the 9 stencil rows it bounds the
+// squared distance from the target to the row in (y, z); rows that cannot
+// hold a partner are skipped, and, when particles are x-sorted within cells
+// (LJ_ORDER_X, so every row of 3 cells is x-sorted), binary search narrows
+// the row to the x-window [x - h, x + h], h = sqrt(rc^2 - dyz^2) plus a
+// rounding slack.  The windows are a superset of the interacting partners,
+// so the shared float distance test alone decides, and the pair count is
+// exact.  Pair math is FP32 from r^-2 (one approximate reciprocal), sums are
+// accumulated in registers, and the totals (energy, virial, pair count) are
+// reduced in FP64 / u64 per block and then by the last block in a fixed
+// order, so they are deterministic.
+#include <cfloat>
+
+#include "ljcell_internal.cuh"
+
+namespace ljc {
+
+struct Partial {
+    double e;
+    double w;
+    unsigned long long p;
+    unsigned long long pad;
+};
+
+struct PairParams {
+    float rc2;     // cutoff^2 (float), the distance test threshold
+    float rc2w;    // rc2 * (1 + 1e-5): window / row-skip bound, above any rounding of the test
+    float sig2;    // sigma^2
+    float e4;      // 4 eps
+    float e24;     // 24 eps
+    float slack;   // absolute rounding slack for cell planes and window ends
+};
+
+__device__ __forceinline__ void decode_cell(const GridDev& g, int c, int& cx, int& cy, int& cz) {
+    const int gxy = g.gx * g.gy;
+    cz = c / gxy;
+    const int r = c - cz * gxy;
+    cy = r / g.gx;
+    cx = r - cy * g.gx;
+}
+
+// first j in [lo, hi) with p[j].x >= v (x-sorted range)
+__device__ __forceinline__ int lower_x(const float4* __restrict__ p, int lo, int hi, float v) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&p[mid].x) < v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+// first j in [lo, hi) with p[j].x > v
+__device__ __forceinline__ int upper_x(const float4* __restrict__ p, int lo, int hi, float v) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&p[mid].x) <= v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+constexpr int kPairThreads = 128;
+constexpr int kMaxWin = 10;
+
+// Block reduction of the totals followed by a last-block final pass.
+__device__ void reduce_totals(double e, double w, unsigned long long np, Partial* part, unsigned* counter,
+                              lj_totals* totals) {
+    __shared__ double s_e[kPairThreads / 32], s_w[kPairThreads / 32];
+    __shared__ unsigned long long s_p[kPairThreads / 32];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    e = warp_sum(e);
+    w = warp_sum(w);
+    np = warp_sum(np);
+    if (lane == 0) {
+        s_e[warp] = e;
+        s_w[warp] = w;
+        s_p[warp] = np;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double te = 0, tw = 0;
+        unsigned long long tp = 0;
+        for (int i = 0; i < kPairThreads / 32; ++i) {
+            te += s_e[i];
+            tw += s_w[i];
+            tp += s_p[i];
+        }
+        part[blockIdx.x] = Partial{te, tw, tp, 0ULL};
+        __threadfence();
+        const unsigned done = atomicAdd(counter, 1u);
+        s_last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double te = 0, tw = 0;
+    unsigned long long tp = 0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        const volatile Partial* q = part + b;
+        te += q->e;
+        tw += q->w;
+        tp += q->p;
+    }
+    te = warp_sum(te);
+    tw = warp_sum(tw);
+    tp = warp_sum(tp);
+    __syncthreads();
+    if (lane == 0) {
+        s_e[warp] = te;
+        s_w[warp] = tw;
+        s_p[warp] = tp;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double fe = 0, fw = 0;
+        unsigned long long fp = 0;
+        for (int i = 0; i < kPairThreads / 32; ++i) {
+            fe += s_e[i];
+            fw += s_w[i];
+            fp += s_p[i];
+        }
+        if (totals) {
+            totals->energy = fe;
+            totals->virial = fw;
+            totals->pairs = fp;
+            totals->pad = 0ULL;
+        }
+        *counter = 0u;  // ready for the next launch
+    }
+}
+
+template <bool XWIN>
+__global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairParams pp, const float4* __restrict__ p,
+                                                              const int* __restrict__ cs,
+                                                              const int* __restrict__ off, int n,
+                                                              float* __restrict__ energy, float* __restrict__ force,
+                                                              Partial* part, unsigned* counter, lj_totals* totals,
+                                                              unsigned* status) {
+    __shared__ int2 s_win[kMaxWin][kPairThreads];
+    const int tid = threadIdx.x;
+    const int k = blockIdx.x * kPairThreads + tid;
+    float ea = 0.f, fx = 0.f, fy = 0.f, fz = 0.f, wa = 0.f;
+    unsigned np = 0;
+    if (k < n) {
+        const float4 pi = p[k];
+        int c = cs[k];
+        const int ncell = g.gx * g.gy * g.gz;
+        if (c < 0 || c >= ncell) {
+            atomicOr(status, kFlagRange);
+            c = 0;
+        }
+        int cx, cy, cz;
+        decode_cell(g, c, cx, cy, cz);
+        const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
+        const float slack =
+            pp.slack + 8.0f * FLT_EPSILON * fmaxf(fabsf(pi.x), fmaxf(fabsf(pi.y), fabsf(pi.z)));
+        int nw = 0;
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int z = cz + dz;
+            if (z < 0 || z >= g.gz) continue;
+            float dzm = 0.f;
+            if (XWIN) {
+                if (dz < 0) dzm = pi.z - fmaf((float)cz, g.w, g.oz);
+                if (dz > 0) dzm = fmaf((float)(cz + 1), g.w, g.oz) - pi.z;
+                dzm = fmaxf(dzm - slack, 0.f);
+            }
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = cy + dy;
+                if (y < 0 || y >= g.gy) continue;
+                const int rb = (z * g.gy + y) * g.gx;
+                int s = min(max(__ldg(&off[rb + xl]), 0), n);
+                int e = min(max(__ldg(&off[rb + xh + 1]), s), n);
+                if (XWIN) {
+                    float dym = 0.f;
+                    if (dy < 0) dym = pi.y - fmaf((float)cy, g.w, g.oy);
+                    if (dy > 0) dym = fmaf((float)(cy + 1), g.w, g.oy) - pi.y;
+                    dym = fmaxf(dym - slack, 0.f);
+                    const float d2 = fmaf(dym, dym, dzm * dzm);
+                    if (d2 >= pp.rc2w) continue;
+                    const float h = sqrtf(pp.rc2w - d2) + slack;
+                    s = lower_x(p, s, e, pi.x - h);
+                    e = upper_x(p, s, e, pi.x + h);
+                }
+                if (dz == 0 && dy == 0) {
+                    s_win[nw++][tid] = make_int2(s, k);
+                    s_win[nw++][tid] = make_int2(k + 1, e);
+                } else {
+                    s_win[nw++][tid] = make_int2(s, e);
+                }
+            }
+        }
+        int w = 0;
+        int2 cur = s_win[0][tid];
+        const float rc2 = pp.rc2, sig2 = pp.sig2;
+        while (true) {
+            while (cur.x >= cur.y) {
+                if (++w >= nw) goto done;
+                cur = s_win[w][tid];
+            }
+            {
+                const float4 q = __ldg(&p[cur.x]);
+                ++cur.x;
+                const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                if (r2 < rc2) {
+                    const float ir2 = rcp_approx(r2);
+                    const float s2 = sig2 * ir2;
+                    const float s6 = s2 * s2 * s2;
+                    const float s12 = s6 * s6;
+                    ea += s12 - s6;
+                    const float t = fmaf(2.0f, s12, -s6);
+                    wa += t;
+                    const float fs = ir2 * t;
+                    fx = fmaf(fs, dx, fx);
+                    fy = fmaf(fs, dy, fy);
+                    fz = fmaf(fs, dz, fz);
+                    ++np;
+                }
+            }
+        }
+    done:
+        if (energy) energy[k] = pp.e4 * ea;
+        if (force) {
+            force[3 * (size_t)k + 0] = -pp.e24 * fx;
+            force[3 * (size_t)k + 1] = -pp.e24 * fy;
+            force[3 * (size_t)k + 2] = -pp.e24 * fz;
+        }
+    }
+    reduce_totals(0.5 * (double)pp.e4 * (double)ea, 0.5 * (double)pp.e24 * (double)wa, (unsigned long long)np, part,
+                  counter, totals);
+}
+
+__global__ void __launch_bounds__(kPairThreads) k_pair_compat(GridDev g, const float4* __restrict__ p,
+                                                              const int* __restrict__ cs,
+                                                              const int* __restrict__ off, int n,
+                                                              float* __restrict__ v, unsigned* status) {
+    const int k = blockIdx.x * kPairThreads + threadIdx.x;
+    if (k >= n) return;
+    const float4 pi = p[k];
+    int c = cs[k];
+    if (c < 0 || c >= g.gx * g.gy * g.gz) {
+        atomicOr(status, kFlagRange);
+        c = 0;
+    }
+    int cx, cy, cz;
+    decode_cell(g, c, cx, cy, cz);
+    const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
+    float pot = 0.f;
+    for (int z = max(cz - 1, 0); z <= min(cz + 1, g.gz - 1); ++z)
+        for (int y = max(cy - 1, 0); y <= min(cy + 1, g.gy - 1); ++y) {
+            const int rb = (z * g.gy + y) * g.gx;
+            const int s = min(max(__ldg(&off[rb + xl]), 0), n);
+            const int e = min(max(__ldg(&off[rb + xh + 1]), s), n);
+            for (int j = s; j < e; ++j) {
+                if (j == k) continue;
+                const float4 q = __ldg(&p[j]);
+                const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+                const float r = sqrtf(dx * dx + dy * dy + dz * dz + 1e-5f);
+                const float sdr = 1.0f / r;
+                const float r6 = (sdr * sdr) * (sdr * sdr) * (sdr * sdr);
+                const float r12 = r6 * r6;
+                pot += 4.0f * (r12 - r6);
+            }
+        }
+    v[k] = pot;
+}
+
+static float grid_slack(const lj_grid& g) {
+    float m = 0.f;
+    for (int d = 0; d < 3; ++d) {
+        const float a = fabsf(g.origin[d]) + (float)g.dim[d] * g.width;
+        m = a > m ? a : m;
+    }
+    return 8.0f * FLT_EPSILON * (m + g.width) + 1e-30f;
+}
+
+lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm, int n, const float* xyzi,
+                             const int* cs, const int* off, lj_order order, float* energy, float* force,
+                             lj_totals* totals) {
+    const int blocks = (n + kPairThreads - 1) / kPairThreads;
+    const size_t need = 256 + (size_t)(blocks > 0 ? blocks : 1) * sizeof(Partial);
+    if (need > ctx->red_bytes) {
+        lj_status s = grow(&ctx->red, &ctx->red_bytes, need);
+        if (s != LJ_OK) return s;
+        if (cudaMemsetAsync(ctx->red, 0, 256, ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    }
+    if (n == 0) {
+        if (totals && cudaMemsetAsync(totals, 0, sizeof(lj_totals), ctx->stream) != cudaSuccess) return LJ_ECUDA;
+        return LJ_OK;
+    }
+    PairParams pp;
+    pp.rc2 = prm->cutoff * prm->cutoff;
+    pp.rc2w = pp.rc2 * (1.0f + 1e-5f);
+    pp.sig2 = prm->sigma * prm->sigma;
+    pp.e4 = 4.0f * prm->epsilon;
+    pp.e24 = 24.0f * prm->epsilon;
+    pp.slack = grid_slack(*g);
+    unsigned* counter = static_cast<unsigned*>(ctx->red);
+    Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
+    const float4* p4 = reinterpret_cast<const float4*>(xyzi);
+    if (order == LJ_ORDER_X)
+        k_pair_config<true><<<blocks, kPairThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, energy, force,
+                                                                      part, counter, totals, ctx->d_status);
+    else
+        k_pair_config<false><<<blocks, kPairThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, energy,
+                                                                       force, part, counter, totals, ctx->d_status);
+    return last_launch_status();
+}
+
+}  // namespace ljc
+
+using namespace ljc;
+
+extern "C" lj_status lj_compute_compat(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi,
+                                       const int* sorted_cell, const int* offsets, float* v) {
+    if (!ctx || !g || n < 0 || (n > 0 && (!sorted_xyzi || !sorted_cell || !offsets || !v))) return LJ_EINVAL;
+    if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
+    if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
+    if (n == 0) return LJ_OK;
+    k_pair_compat<<<(n + kPairThreads - 1) / kPairThreads, kPairThreads, 0, ctx->stream>>>(
+        to_dev(*g), reinterpret_cast<const float4*>(sorted_xyzi), sorted_cell, offsets, n, v, ctx->d_status);
+    return last_launch_status();
+}
+
+extern "C" lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* sorted_xyzi,
+                                const int* sorted_cell, const int* offsets, lj_order order, float* energy,
+                                float* force, lj_totals* totals) {
+    if (!ctx || !g || !p || n < 0) return LJ_EINVAL;
+    if (n > 0 && (!sorted_xyzi || !sorted_cell || !offsets)) return LJ_EINVAL;
+    if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
+    if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width)) return LJ_EINVAL;
+    if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
+    if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
+    return launch_pair_config(ctx, g, p, n, sorted_xyzi, sorted_cell, offsets, order, energy, force, totals);
+}

@@ -1,0 +1,324 @@
+"""ljcell -- Python host layer over the C ABI of the B200 cell-grid LJ path.
+
+This mirrors the reference's step (OptixLJ Cuda-version/cudaLJ.cu,
+executeSimulation at cudaLJ.cu:515-677): generation, the cell-grid build
+(count, scan, descriptors, scatter), the candidate count and the pair
+kernel, each a call into libljcell.so (include/ljcell.h).  PyTorch provides
+device memory and streams only; every computation runs in the library's own
+sm_100a kernels.  There is no CPU fallback: importing this package on a
+machine where libljcell.so cannot be loaded raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libljcell.so")
+
+LJ_OK, LJ_EINVAL, LJ_ENOMEM, LJ_ECUDA, LJ_ETIMEOUT, LJ_ERANGE, LJ_EUNSUPPORTED = range(7)
+ORDER_INDEX = 0
+ORDER_X = 1
+
+
+class Grid(C.Structure):
+    """lj_grid: origin, cell width, dims (x fastest)."""
+
+    _fields_ = [("origin", C.c_float * 3), ("width", C.c_float), ("dim", C.c_int * 3)]
+
+    @property
+    def ncells(self) -> int:
+        return int(self.dim[0]) * int(self.dim[1]) * int(self.dim[2])
+
+    def __repr__(self):
+        return (f"Grid(origin={tuple(self.origin)}, width={self.width}, dim={tuple(self.dim)})")
+
+
+class Params(C.Structure):
+    """lj_params: truncated LJ cutoff, epsilon, sigma."""
+
+    _fields_ = [("cutoff", C.c_float), ("epsilon", C.c_float), ("sigma", C.c_float)]
+
+
+class Totals(C.Structure):
+    """lj_totals: E = 1/2 sum e_i, virial, interacting ordered pairs."""
+
+    _fields_ = [("energy", C.c_double), ("virial", C.c_double), ("pairs", C.c_ulonglong), ("pad", C.c_ulonglong)]
+
+
+class Particles(C.Structure):
+    """lj_particles == ParticlesContainer<float> (cudaLJ.cu:60-67)."""
+
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("v", C.c_void_p),
+                ("index", C.c_void_p), ("nbParticles", C.c_int)]
+
+
+class LJError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        super().__init__(f"{where}: {status_str(status)} (status {status})")
+        self.status = status
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libljcell.so not built at {LIB_PATH}; run __graft_entry__.build() or "
+                          f"`make -C particle-interaction-with-optix_b200/csrc`")
+    lib = C.CDLL(LIB_PATH)
+    vp, i32, i64, f32 = C.c_void_p, C.c_int, C.c_longlong, C.c_float
+    f3 = C.POINTER(C.c_float)
+    sig = {
+        "lj_abi_version": (C.c_int, []),
+        "lj_status_str": (C.c_char_p, [i32]),
+        "lj_create": (i32, [C.POINTER(vp), i32, vp]),
+        "lj_destroy": (i32, [vp]),
+        "lj_set_stream": (i32, [vp, vp]),
+        "lj_sync": (i32, [vp]),
+        "lj_generate_uniform": (i32, [vp, C.c_uint64, i32, f3, f3, C.POINTER(Particles), vp]),
+        "lj_generate_sphere": (i32, [vp, C.c_uint64, i32, f3, f32, C.POINTER(Particles), vp]),
+        "lj_grid_from_box": (i32, [f3, f3, f32, C.POINTER(Grid)]),
+        "lj_grid_compat": (i32, [f32, f32, C.POINTER(Grid)]),
+        "lj_count_cells": (i32, [vp, C.POINTER(Grid), i32, vp, vp, vp, i32, vp]),
+        "lj_exclusive_scan": (i32, [vp, vp, i64, vp]),
+        "lj_cell_descriptors": (i32, [vp, vp, i64, vp]),
+        "lj_bin": (i32, [vp, C.POINTER(Grid), i32, vp, vp, vp, i32, i32, vp, vp, vp, C.POINTER(Particles), vp, vp]),
+        "lj_count_candidates": (i32, [vp, C.POINTER(Grid), vp, vp]),
+        "lj_compute_compat": (i32, [vp, C.POINTER(Grid), i32, vp, vp, vp, vp]),
+        "lj_compute": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, i32, vp, vp, vp]),
+        "lj_simulate_host": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
+                                   C.POINTER(Totals)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_lib = _load()
+ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj_set_stream", "lj_sync",
+               "lj_generate_uniform", "lj_generate_sphere", "lj_grid_from_box", "lj_grid_compat",
+               "lj_count_cells", "lj_exclusive_scan", "lj_cell_descriptors", "lj_bin", "lj_count_candidates",
+               "lj_compute_compat", "lj_compute", "lj_simulate_host")
+
+
+def lib() -> C.CDLL:
+    return _lib
+
+
+def status_str(s: int) -> str:
+    return _lib.lj_status_str(s).decode()
+
+
+def _check(s: int, where: str):
+    if s != LJ_OK:
+        raise LJError(s, where)
+
+
+def _f3(v):
+    return (C.c_float * 3)(*[float(a) for a in v])
+
+
+def grid_from_box(lo, hi, cutoff: float) -> Grid:
+    g = Grid()
+    _check(_lib.lj_grid_from_box(_f3(lo), _f3(hi), cutoff, C.byref(g)), "lj_grid_from_box")
+    return g
+
+
+def grid_compat(box_width: float, cutoff: float) -> Grid:
+    g = Grid()
+    _check(_lib.lj_grid_compat(box_width, cutoff, C.byref(g)), "lj_grid_compat")
+    return g
+
+
+def default_sigma(cutoff: float) -> float:
+    """sigma = r_c / 2.5 evaluated in float32."""
+    return float(np.float32(cutoff) / np.float32(2.5))
+
+
+def params(cutoff: float, epsilon: float = 1.0, sigma: float | None = None) -> Params:
+    return Params(cutoff, epsilon, default_sigma(cutoff) if sigma is None else sigma)
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+@dataclass
+class Binned:
+    """Device buffers of one binned system (torch tensors)."""
+    n: int
+    order: int
+    counts: object
+    offsets: object
+    xyzi: object           # (n, 4) float32: x, y, z, original index bits
+    cell: object           # (n,) int32
+    sx: object | None = None
+    sy: object | None = None
+    sz: object | None = None
+    index: object | None = None
+    cells: object | None = None   # (ncells, 2) int32 CellDescriptor view
+
+
+class Context:
+    """An lj_ctx bound to one device and one stream."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        h = C.c_void_p()
+        s = None if stream is None else C.c_void_p(stream.cuda_stream)
+        _check(_lib.lj_create(C.byref(h), device, s), "lj_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lj_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream):
+        _check(_lib.lj_set_stream(self._h, None if stream is None else C.c_void_p(stream.cuda_stream)),
+               "lj_set_stream")
+
+    def sync(self):
+        _check(_lib.lj_sync(self._h), "lj_sync")
+
+    # ------------------------------------------------------------ generation
+    def _gen_out(self, n, want_soa, want_aos):
+        t = self.torch
+        soa = None
+        if want_soa:
+            soa = {k: t.empty(n, dtype=t.float32, device=self.device) for k in ("x", "y", "z", "v")}
+            soa["index"] = t.empty(n, dtype=t.int32, device=self.device)
+        aos = t.empty((n, 3), dtype=t.float32, device=self.device) if want_aos else None
+        p = Particles()
+        if soa:
+            p.x, p.y, p.z, p.v, p.index = (soa[k].data_ptr() for k in ("x", "y", "z", "v", "index"))
+        p.nbParticles = n
+        return soa, aos, p
+
+    def generate_uniform(self, seed: int, n: int, lo=(0, 0, 0), hi=(1, 1, 1), soa=True, aos=False):
+        s, a, p = self._gen_out(n, soa, aos)
+        _check(_lib.lj_generate_uniform(self._h, seed, n, _f3(lo), _f3(hi), C.byref(p), _ptr(a)),
+               "lj_generate_uniform")
+        return s, a
+
+    def generate_sphere(self, seed: int, n: int, centre=(0.5, 0.5, 0.5), radius=1.0, soa=True, aos=False):
+        s, a, p = self._gen_out(n, soa, aos)
+        _check(_lib.lj_generate_sphere(self._h, seed, n, _f3(centre), radius, C.byref(p), _ptr(a)),
+               "lj_generate_sphere")
+        return s, a
+
+    # ------------------------------------------------------------ binning
+    def alloc_binned(self, g: Grid, n: int, order: int = ORDER_X, soa: bool = False, cells: bool = False) -> Binned:
+        t = self.torch
+        dev = self.device
+        b = Binned(n, order, t.empty(g.ncells, dtype=t.int32, device=dev),
+                   t.empty(g.ncells + 1, dtype=t.int32, device=dev),
+                   t.empty((max(n, 1), 4), dtype=t.float32, device=dev),
+                   t.empty(max(n, 1), dtype=t.int32, device=dev))
+        if soa:
+            b.sx, b.sy, b.sz = (t.empty(max(n, 1), dtype=t.float32, device=dev) for _ in range(3))
+            b.index = t.empty(max(n, 1), dtype=t.int32, device=dev)
+        if cells:
+            b.cells = t.empty((g.ncells, 2), dtype=t.int32, device=dev)
+        return b
+
+    def bin(self, g: Grid, x, y, z, stride: int = 1, order: int = ORDER_X, out: Binned | None = None,
+            soa: bool = False, cells: bool = False) -> Binned:
+        n = int(x.numel()) // stride if stride > 1 else int(x.numel())
+        b = out if out is not None else self.alloc_binned(g, n, order, soa, cells)
+        b.order = order
+        sp = None
+        if b.sx is not None or b.index is not None:
+            sp = Particles(None if b.sx is None else b.sx.data_ptr(), None if b.sy is None else b.sy.data_ptr(),
+                           None if b.sz is None else b.sz.data_ptr(), None,
+                           None if b.index is None else b.index.data_ptr(), n)
+        _check(_lib.lj_bin(self._h, C.byref(g), n, _ptr(x), _ptr(y), _ptr(z), stride, order, _ptr(b.counts),
+                           _ptr(b.offsets), _ptr(b.cells), C.byref(sp) if sp is not None else None, _ptr(b.xyzi),
+                           _ptr(b.cell)), "lj_bin")
+        return b
+
+    def count_cells(self, g: Grid, x, y, z, stride: int = 1, counts=None):
+        t = self.torch
+        n = int(x.numel()) // stride if stride > 1 else int(x.numel())
+        counts = counts if counts is not None else t.empty(g.ncells, dtype=t.int32, device=self.device)
+        _check(_lib.lj_count_cells(self._h, C.byref(g), n, _ptr(x), _ptr(y), _ptr(z), stride, _ptr(counts)),
+               "lj_count_cells")
+        return counts
+
+    def exclusive_scan(self, counts, offsets=None):
+        t = self.torch
+        nc = int(counts.numel())
+        offsets = offsets if offsets is not None else t.empty(nc + 1, dtype=t.int32, device=self.device)
+        _check(_lib.lj_exclusive_scan(self._h, _ptr(counts), nc, _ptr(offsets)), "lj_exclusive_scan")
+        return offsets
+
+    def cell_descriptors(self, offsets, cells=None):
+        t = self.torch
+        nc = int(offsets.numel()) - 1
+        cells = cells if cells is not None else t.empty((nc, 2), dtype=t.int32, device=self.device)
+        _check(_lib.lj_cell_descriptors(self._h, _ptr(offsets), nc, _ptr(cells)), "lj_cell_descriptors")
+        return cells
+
+    # ------------------------------------------------------------ interactions
+    def count_candidates(self, g: Grid, offsets, out=None):
+        t = self.torch
+        out = out if out is not None else t.empty(1, dtype=t.int64, device=self.device)
+        _check(_lib.lj_count_candidates(self._h, C.byref(g), _ptr(offsets), _ptr(out)), "lj_count_candidates")
+        return out
+
+    def compute_compat(self, g: Grid, b: Binned, v=None):
+        t = self.torch
+        v = v if v is not None else t.empty(max(b.n, 1), dtype=t.float32, device=self.device)
+        _check(_lib.lj_compute_compat(self._h, C.byref(g), b.n, _ptr(b.xyzi), _ptr(b.cell), _ptr(b.offsets),
+                                      _ptr(v)), "lj_compute_compat")
+        return v
+
+    def alloc_outputs(self, n: int):
+        t = self.torch
+        e = t.empty(max(n, 1), dtype=t.float32, device=self.device)
+        f = t.empty((max(n, 1), 3), dtype=t.float32, device=self.device)
+        tot = t.zeros(4, dtype=t.float64, device=self.device)  # one lj_totals (32 bytes)
+        return e, f, tot
+
+    def compute(self, g: Grid, p: Params, b: Binned, energy=None, force=None, totals=None, want_energy=True,
+                want_force=True):
+        if energy is None and force is None and totals is None:
+            energy, force, totals = self.alloc_outputs(b.n)
+        _check(_lib.lj_compute(self._h, C.byref(g), C.byref(p), b.n, _ptr(b.xyzi), _ptr(b.cell), _ptr(b.offsets),
+                               b.order, _ptr(energy) if want_energy else None,
+                               _ptr(force) if want_force else None, _ptr(totals)), "lj_compute")
+        return energy, force, totals
+
+    def simulate_host(self, g: Grid, p: Params, hx: np.ndarray, hy: np.ndarray, hz: np.ndarray,
+                      energy: np.ndarray | None = None, force: np.ndarray | None = None,
+                      index: np.ndarray | None = None):
+        n = len(hx)
+        tot = Totals()
+        fp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        _check(_lib.lj_simulate_host(self._h, C.byref(g), C.byref(p), n, fp(hx), fp(hy), fp(hz), fp(energy),
+                                     fp(force), fp(index), C.byref(tot)), "lj_simulate_host")
+        return tot
+
+
+def totals_from_tensor(tot) -> dict:
+    """Decodes one lj_totals held in a 4-element float64 tensor."""
+    raw = tot.detach().cpu().numpy().view(np.uint8).tobytes()
+    e, w = np.frombuffer(raw[:16], np.float64)
+    pairs = int(np.frombuffer(raw[16:24], np.uint64)[0])
+    return {"energy": float(e), "virial": float(w), "pairs": pairs}

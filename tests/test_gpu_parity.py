@@ -1,0 +1,322 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the CPU
+oracle on the same seeded inputs.  Integer and index outputs (generation of
+the uniform box, counts, offsets, permutation, cell ids, descriptors,
+candidate and interacting-pair counts) must be bit-exact; floating-point
+outputs are held to the tolerances stated in each test."""
+import numpy as np
+import pytest
+
+import ljoracle as O
+
+pytestmark = pytest.mark.gpu
+
+# FP32 pair math against the FP64 oracle: error relative to each particle's
+# conditioning scale (sum of the pair terms' magnitudes before cancellation).
+FORCE_SCALED_TOL = 1e-5
+ENERGY_SCALED_TOL = 1e-5
+FORCE_NORMWISE_TOL = 1e-5     # ||F - F64|| / ||F64|| over all particles
+TOTAL_ENERGY_TOL = 1e-6       # |E - E64| / |E64|
+COMPAT_REL_TOL = 1e-5         # reference tolerance, cudaLJ.cu:246-250
+
+
+def np_(t):
+    return t.detach().cpu().numpy()
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+# ------------------------------------------------------------------ inputs
+def case_positions(name):
+    if name == "uniform_c1":
+        x, y, z = O.generate_uniform(1234, 100_000)
+        return (x, y, z), ((0, 0, 0), (1, 1, 1)), 0.05
+    if name == "uniform_dense":
+        x, y, z = O.generate_uniform(77, 60_000)
+        return (x, y, z), ((0, 0, 0), (1, 1, 1)), 0.1
+    if name == "shell":
+        x, y, z = O.generate_sphere(1234, 150_000, (0.5, 0.5, 0.5), 1.0)
+        return (x, y, z), ((-0.5,) * 3, (1.5,) * 3), 0.01
+    if name == "clustered":
+        # one cell holds 5000 particles (beyond the warp sort), plus background
+        rng = np.random.default_rng(5)
+        a = rng.random((5000, 3), dtype=np.float32) * np.float32(0.01) + np.float32(0.4)
+        b = rng.random((20000, 3), dtype=np.float32)
+        p = np.concatenate([a, b]).astype(np.float32)
+        return (p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy()), ((0, 0, 0), (1, 1, 1)), 0.05
+    if name == "outside_and_faces":
+        rng = np.random.default_rng(9)
+        w = np.float32(0.0625)
+        faces = np.unique((rng.integers(0, 17, (3000, 3)) * w).astype(np.float32), axis=0)  # no coincident pairs
+        out = (rng.random((500, 3)) * 1.6 - 0.3).astype(np.float32)
+        inner = rng.random((8000, 3), dtype=np.float32)
+        p = np.concatenate([faces, out, inner]).astype(np.float32)
+        return (p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy()), ((0, 0, 0), (1, 1, 1)), float(w)
+    if name.startswith("tiny"):
+        n = int(name[4:])
+        x, y, z = O.generate_uniform(3, n)
+        return (x, y, z), ((0, 0, 0), (1, 1, 1)), 0.25
+    raise KeyError(name)
+
+
+BIN_CASES = ["uniform_c1", "uniform_dense", "shell", "clustered", "outside_and_faces", "tiny1", "tiny2", "tiny33"]
+
+
+def bin_both(torch, ctx, name, order, stride=1):
+    import ljcell
+
+    (x, y, z), (lo, hi), rc = case_positions(name)
+    g = ljcell.grid_from_box(lo, hi, rc)
+    og = O.grid_from_box(lo, hi, rc)
+    if stride == 3:
+        aos = dev(torch, np.stack([x, y, z], axis=1).reshape(-1))
+        b = ctx.bin(g, aos, aos[1:], aos[2:], stride=3, order=order, out=ctx.alloc_binned(g, len(x), order, True,
+                                                                                             True))
+    else:
+        b = ctx.bin(g, dev(torch, x), dev(torch, y), dev(torch, z), order=order, soa=True, cells=True)
+    ctx.sync()
+    ob = O.bin_particles(og, x, y, z, order)
+    return (x, y, z), g, og, b, ob, rc
+
+
+# ------------------------------------------------------------------ generation
+def test_generate_uniform_bit_exact(ctx):
+    n = 100_003
+    soa, aos = ctx.generate_uniform(1234, n, aos=True)
+    ctx.sync()
+    x, y, z = O.generate_uniform(1234, n)
+    np.testing.assert_array_equal(np_(soa["x"]), x)
+    np.testing.assert_array_equal(np_(soa["y"]), y)
+    np.testing.assert_array_equal(np_(soa["z"]), z)
+    np.testing.assert_array_equal(np_(aos), np.stack([x, y, z], 1))
+    np.testing.assert_array_equal(np_(soa["index"]), np.arange(n, dtype=np.int32))
+    assert np.all(np_(soa["v"]) == -1.0)
+
+
+def test_generate_uniform_box_bit_exact(ctx):
+    soa, _ = ctx.generate_uniform(99, 5000, lo=(-0.5, 0.25, 2.0), hi=(1.5, 0.75, 3.0))
+    ctx.sync()
+    x, y, z = O.generate_uniform(99, 5000, (-0.5, 0.25, 2.0), (1.5, 0.75, 3.0))
+    np.testing.assert_array_equal(np_(soa["x"]), x)
+    np.testing.assert_array_equal(np_(soa["z"]), z)
+
+
+def test_generate_sphere_within_one_ulp(ctx):
+    n = 50_000
+    soa, _ = ctx.generate_sphere(1234, n, (0.5, 0.5, 0.5), 1.0)
+    ctx.sync()
+    ref = O.generate_sphere(1234, n, (0.5, 0.5, 0.5), 1.0)
+    for k, r in zip("xyz", ref):
+        d = np.abs(np_(soa[k]).astype(np.float64) - r.astype(np.float64))
+        assert np.all(d <= np.spacing(np.abs(r)).astype(np.float64)), k
+
+
+# ------------------------------------------------------------------ scan
+@pytest.mark.parametrize("ncells", [1, 5, 4095, 4096, 4097, 123_457, 1_000_000, 64_000_000])
+def test_exclusive_scan(torch_cuda, ctx, ncells):
+    torch = torch_cuda
+    g = torch.Generator(device="cuda").manual_seed(ncells)
+    counts = torch.randint(0, 4, (ncells,), dtype=torch.int32, device="cuda", generator=g)
+    off = ctx.exclusive_scan(counts)
+    ctx.sync()
+    c = np_(counts).astype(np.int64)
+    ref = np.concatenate([[0], np.cumsum(c)])
+    np.testing.assert_array_equal(np_(off).astype(np.int64), ref)
+
+
+def test_exclusive_scan_unaligned(torch_cuda, ctx):
+    torch = torch_cuda
+    base = torch.randint(0, 9, (100_001,), dtype=torch.int32, device="cuda")
+    out = torch.empty(100_002, dtype=torch.int32, device="cuda")
+    off = ctx.exclusive_scan(base[1:], out[1:])
+    ctx.sync()
+    ref = np.concatenate([[0], np.cumsum(np_(base[1:]).astype(np.int64))])
+    np.testing.assert_array_equal(np_(off), ref)
+
+
+def test_scan_matches_reference_semantics(torch_cuda, ctx):
+    # reference: memset prefix, PrefixFullV2(counts, prefix + 1) -> prefix[0] = 0, prefix[i+1] = sum counts[0..i]
+    torch = torch_cuda
+    counts = torch.randint(0, 30, (20 ** 3,), dtype=torch.int32, device="cuda")
+    off = ctx.exclusive_scan(counts)
+    ctx.sync()
+    o = np_(off)
+    assert o[0] == 0 and np.array_equal(np.diff(o), np_(counts))
+
+
+# ------------------------------------------------------------------ binning
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("name", BIN_CASES)
+def test_bin_bit_exact(torch_cuda, ctx, name, order):
+    (x, y, z), g, og, b, ob, _ = bin_both(torch_cuda, ctx, name, order)
+    np.testing.assert_array_equal(np_(b.counts), ob.counts)
+    np.testing.assert_array_equal(np_(b.offsets), ob.offsets)
+    n = len(x)
+    xyzi = np_(b.xyzi)[:n]
+    np.testing.assert_array_equal(xyzi[:, 3].view(np.int32), ob.perm)
+    np.testing.assert_array_equal(xyzi[:, 0], ob.sx)
+    np.testing.assert_array_equal(xyzi[:, 1], ob.sy)
+    np.testing.assert_array_equal(xyzi[:, 2], ob.sz)
+    np.testing.assert_array_equal(np_(b.cell)[:n], ob.cell_sorted)
+    np.testing.assert_array_equal(np_(b.sx)[:n], ob.sx)
+    np.testing.assert_array_equal(np_(b.index)[:n], ob.perm)
+    cells = np_(b.cells)
+    np.testing.assert_array_equal(cells[:, 0], ob.counts)
+    np.testing.assert_array_equal(cells[:, 1], ob.offsets[:-1])
+
+
+@pytest.mark.parametrize("name", ["uniform_c1", "outside_and_faces"])
+def test_bin_aos_point3d_input(torch_cuda, ctx, name):
+    (x, y, z), g, og, b, ob, _ = bin_both(torch_cuda, ctx, name, 1, stride=3)
+    np.testing.assert_array_equal(np_(b.offsets), ob.offsets)
+    np.testing.assert_array_equal(np_(b.xyzi)[:len(x), 3].view(np.int32), ob.perm)
+
+
+def test_count_cells_and_descriptors(torch_cuda, ctx):
+    torch = torch_cuda
+    import ljcell
+
+    x, y, z = O.generate_uniform(8, 70_000)
+    g = ljcell.grid_from_box((0, 0, 0), (1, 1, 1), 0.04)
+    og = O.grid_from_box((0, 0, 0), (1, 1, 1), 0.04)
+    counts = ctx.count_cells(g, dev(torch, x), dev(torch, y), dev(torch, z))
+    off = ctx.exclusive_scan(counts)
+    cells = ctx.cell_descriptors(off)
+    ctx.sync()
+    ob = O.bin_particles(og, x, y, z)
+    np.testing.assert_array_equal(np_(counts), ob.counts)
+    np.testing.assert_array_equal(np_(cells)[:, 1], ob.offsets[:-1])
+
+
+def test_bin_empty(torch_cuda, ctx):
+    torch = torch_cuda
+    import ljcell
+
+    g = ljcell.grid_from_box((0, 0, 0), (1, 1, 1), 0.25)
+    e = torch.empty(0, dtype=torch.float32, device="cuda")
+    b = ctx.bin(g, e, e, e)
+    ctx.sync()
+    assert np.all(np_(b.counts) == 0) and np.all(np_(b.offsets) == 0)
+    energy, force, tot = ctx.compute(g, ljcell.params(0.25), b)
+    ctx.sync()
+    assert ljcell.totals_from_tensor(tot)["pairs"] == 0
+
+
+def test_non_finite_position_reported(torch_cuda, ctx):
+    torch = torch_cuda
+    import ljcell
+
+    x, y, z = O.generate_uniform(1, 1000)
+    x[10] = np.nan
+    g = ljcell.grid_from_box((0, 0, 0), (1, 1, 1), 0.1)
+    ctx.bin(g, dev(torch, x), dev(torch, y), dev(torch, z))
+    with pytest.raises(ljcell.LJError) as ei:
+        ctx.sync()
+    assert ei.value.status == ljcell.LJ_ERANGE
+    ctx.sync()  # status word cleared
+
+
+# ------------------------------------------------------------------ candidates / compat law
+@pytest.mark.parametrize("name", ["uniform_c1", "shell", "clustered", "outside_and_faces", "tiny2"])
+def test_candidate_count_exact(torch_cuda, ctx, name):
+    (x, y, z), g, og, b, ob, _ = bin_both(torch_cuda, ctx, name, 1)
+    cnt = ctx.count_candidates(g, b.offsets)
+    ctx.sync()
+    assert int(np_(cnt)[0]) == O.count_candidates(og, ob.offsets)
+
+
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("name", ["uniform_c1", "shell", "outside_and_faces", "tiny33"])
+def test_compat_energy(torch_cuda, ctx, name, order):
+    (x, y, z), g, og, b, ob, _ = bin_both(torch_cuda, ctx, name, order)
+    v = np_(ctx.compute_compat(g, b))[:len(x)]
+    ctx.sync()
+    ref = O.compat_energy(og, ob)
+    rel = np.where(ref == 0, np.abs(v), np.abs((ref - v) / np.where(ref == 0, 1, ref)))
+    assert rel.max() <= COMPAT_REL_TOL
+
+
+# ------------------------------------------------------------------ config law
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("name", ["uniform_c1", "uniform_dense", "shell", "clustered", "outside_and_faces",
+                                  "tiny2", "tiny33"])
+def test_config_forces(torch_cuda, ctx, name, order):
+    import ljcell
+
+    (x, y, z), g, og, b, ob, rc = bin_both(torch_cuda, ctx, name, order)
+    # the cluster packs 5000 particles into 1e-6 volume: a small sigma keeps s^12 inside float range
+    p = ljcell.params(rc, sigma=rc / 500 if name == "clustered" else None)
+    energy, force, tot = ctx.compute(g, p, b)
+    ctx.sync()
+    n = len(x)
+    t = ljcell.totals_from_tensor(tot)
+    ref = O.config_forces(og, ob, rc, 1.0, p.sigma)
+    assert t["pairs"] == ref.pairs
+    e = np_(energy)[:n]
+    f = np_(force)[:n]
+    fe = ref.force_errors(f)
+    ee = ref.energy_errors(e)
+    assert fe["max_scaled"] <= FORCE_SCALED_TOL, fe
+    assert fe["normwise"] <= FORCE_NORMWISE_TOL, fe
+    assert ee["max_scaled"] <= ENERGY_SCALED_TOL, ee
+    if ref.pairs:
+        assert abs(t["energy"] - ref.etot) <= TOTAL_ENERGY_TOL * abs(ref.etot), (t["energy"], ref.etot)
+        assert abs(t["virial"] - ref.virial) <= TOTAL_ENERGY_TOL * abs(ref.virial) + 1e-300
+        assert abs(t["energy"] - 0.5 * e.astype(np.float64).sum()) <= 1e-12 * abs(ref.etot) + 1e-300
+
+
+def test_config_tiny_cutoff_pair_count(torch_cuda, ctx):
+    # small cutoff relative to coordinates: the window slack must still keep every partner
+    import ljcell
+
+    torch = torch_cuda
+    rng = np.random.default_rng(12)
+    base = rng.random((20000, 3)).astype(np.float32) * np.float32(0.02) + np.float32(100.0)
+    x, y, z = (base[:, i].copy() for i in range(3))
+    lo, hi, rc = (100.0, 100.0, 100.0), (100.02, 100.02, 100.02), 0.0008
+    g = ljcell.grid_from_box(lo, hi, rc)
+    og = O.grid_from_box(lo, hi, rc)
+    b = ctx.bin(g, dev(torch, x), dev(torch, y), dev(torch, z), order=1)
+    _, _, tot = ctx.compute(g, ljcell.params(rc), b)
+    ctx.sync()
+    ob = O.bin_particles(og, x, y, z, 1)
+    ref = O.config_forces(og, ob, rc)
+    assert ljcell.totals_from_tensor(tot)["pairs"] == ref.pairs
+
+
+def test_deterministic(torch_cuda, ctx):
+    import ljcell
+
+    torch = torch_cuda
+    (x, y, z), (lo, hi), rc = case_positions("uniform_c1")
+    g = ljcell.grid_from_box(lo, hi, rc)
+    outs = []
+    for _ in range(2):
+        b = ctx.bin(g, dev(torch, x), dev(torch, y), dev(torch, z), order=1)
+        e, f, tot = ctx.compute(g, ljcell.params(rc), b)
+        ctx.sync()
+        outs.append((np_(b.xyzi), np_(e), np_(f), np_(tot)))
+    for a, c in zip(*outs):
+        assert np.array_equal(a.view(np.uint8), c.view(np.uint8))
+
+
+def test_simulate_host_matches_device_path(torch_cuda, ctx):
+    import ljcell
+
+    torch = torch_cuda
+    (x, y, z), (lo, hi), rc = case_positions("uniform_c1")
+    n = len(x)
+    g = ljcell.grid_from_box(lo, hi, rc)
+    p = ljcell.params(rc)
+    he = np.empty(n, np.float32)
+    hf = np.empty((n, 3), np.float32)
+    hi_ = np.empty(n, np.int32)
+    tot = ctx.simulate_host(g, p, x, y, z, he, hf, hi_)
+    b = ctx.bin(g, dev(torch, x), dev(torch, y), dev(torch, z), order=1)
+    e, f, t2 = ctx.compute(g, p, b)
+    ctx.sync()
+    np.testing.assert_array_equal(he, np_(e)[:n])
+    np.testing.assert_array_equal(hf, np_(f)[:n])
+    np.testing.assert_array_equal(hi_, np_(b.xyzi)[:n, 3].view(np.int32))
+    assert tot.pairs == ljcell.totals_from_tensor(t2)["pairs"]
