@@ -405,7 +405,11 @@ def reference_gpu(cfg, x, y, z, ctx, g):
     if not O.ref_available() or cfg["dist"] != "uniform" or tuple(cfg["lo"]) != (0, 0, 0):
         return None
     box = float(cfg["hi"][0])
+    w = np.float32(cfg["rc"])
+    G = int(np.float32(box) / w)
     below = np.nextafter(np.float32(box), np.float32(0))
+    while np.float32(below) / w >= np.float32(G):   # the reference indexes int(x / w) without clamping
+        below = np.nextafter(below, np.float32(0))
     hx, hy, hz = (np.minimum(t.detach().cpu().numpy(), below).astype(np.float32) for t in (x, y, z))
     r = O.ref_run(hx, hy, hz, box, cfg["rc"], reps=3)
     ms = r.stage_ms

@@ -273,6 +273,9 @@ LJO_EXPORT void ljo_compat_energy(const ljo_grid* g, int64_t n, const float* sx,
 /* F_i = 24 eps sum_j r^-2 (2 s^12 - s^6) (p_i - p_j).  Totals:              */
 /* E = 1/2 sum_i e_i, virial W = 1/2 sum_i sum_j 24 eps (2 s^12 - s^6),      */
 /* pairs = number of interacting ordered pairs.                              */
+/* The float force is accumulated as sum (2 s^12 - s^6) s^2 d and scaled by */
+/* -24 eps / sigma^2 once, as the GPU kernel does (no overflow of r^-2 t).   */
+/* nnb[k] (optional) = interacting neighbours of particle k.                 */
 /* The loop visits the reference's full 27-cell stencil (cudaLJ.cu:319-337). */
 /* ------------------------------------------------------------------------ */
 static inline int ljo_interacts(float xi, float yi, float zi, float xj, float yj, float zj, float rc2, float* dx,
@@ -287,7 +290,8 @@ static inline int ljo_interacts(float xi, float yi, float zi, float xj, float yj
 LJO_EXPORT void ljo_config_forces(const ljo_grid* g, int64_t n, const float* sx, const float* sy, const float* sz,
                                   const int* cell_sorted, const int* offsets, float rc, float eps, float sigma,
                                   float* e32, float* f32, double* e64, double* f64, uint64_t* pairs_out,
-                                  double* etot_out, double* vir_out, double* escale64, double* fscale64) {
+                                  double* etot_out, double* vir_out, double* escale64, double* fscale64,
+                                  int* nnb) {
     const int gx = g->dim[0], gy = g->dim[1], gz = g->dim[2];
     const float rc2 = rc * rc;
     const float sig2 = sigma * sigma;
@@ -317,7 +321,7 @@ LJO_EXPORT void ljo_config_forces(const ljo_grid* g, int64_t n, const float* sx,
                             const float s6 = s2 * s2 * s2;
                             const float s12 = s6 * s6;
                             ea += s12 - s6;
-                            const float fs = ir2 * (2.0f * s12 - s6);
+                            const float fs = (2.0f * s12 - s6) * s2;
                             fxa += fs * dx;
                             fya += fs * dy;
                             fza += fs * dz;
@@ -346,10 +350,12 @@ LJO_EXPORT void ljo_config_forces(const ljo_grid* g, int64_t n, const float* sx,
         pairs += np;
         if (e32) e32[k] = 4.0f * eps * ea;
         if (f32) {
-            f32[3 * k + 0] = -24.0f * eps * fxa;
-            f32[3 * k + 1] = -24.0f * eps * fya;
-            f32[3 * k + 2] = -24.0f * eps * fza;
+            const float fsc = -24.0f * eps / sig2;
+            f32[3 * k + 0] = fsc * fxa;
+            f32[3 * k + 1] = fsc * fya;
+            f32[3 * k + 2] = fsc * fza;
         }
+        if (nnb) nnb[k] = (int)np;
         const double e4 = 4.0 * (double)eps, e24 = 24.0 * (double)eps;
         if (e64) e64[k] = e4 * ed;
         if (f64) {
@@ -405,7 +411,7 @@ LJO_EXPORT uint64_t ljo_config_forces_f32_range(const ljo_grid* g, int64_t k0, i
                         const float s6 = s2 * s2 * s2;
                         const float s12 = s6 * s6;
                         ea += s12 - s6;
-                        const float fs = ir2 * (2.0f * s12 - s6);
+                        const float fs = (2.0f * s12 - s6) * s2;
                         fxa += fs * dx;
                         fya += fs * dy;
                         fza += fs * dz;
@@ -413,9 +419,10 @@ LJO_EXPORT uint64_t ljo_config_forces_f32_range(const ljo_grid* g, int64_t k0, i
                 }
         pairs += np;
         e32[k] = 4.0f * eps * ea;
-        f32[3 * k + 0] = -24.0f * eps * fxa;
-        f32[3 * k + 1] = -24.0f * eps * fya;
-        f32[3 * k + 2] = -24.0f * eps * fza;
+        const float fsc = -24.0f * eps / sig2;
+        f32[3 * k + 0] = fsc * fxa;
+        f32[3 * k + 1] = fsc * fya;
+        f32[3 * k + 2] = fsc * fza;
     }
     return pairs;
 }

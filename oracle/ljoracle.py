@@ -61,7 +61,7 @@ def _load():
     lib.ljo_config_forces.argtypes = [
         C.POINTER(Grid), C.c_int64, _f32p, _f32p, _f32p, _i32p, _i32p, C.c_float, C.c_float, C.c_float,
         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double),
-        C.POINTER(C.c_double), C.c_void_p, C.c_void_p]
+        C.POINTER(C.c_double), C.c_void_p, C.c_void_p, C.c_void_p]
     lib.ljo_config_forces_f32_range.restype = C.c_uint64
     lib.ljo_config_forces_f32_range.argtypes = [
         C.POINTER(Grid), C.c_int64, C.c_int64, _f32p, _f32p, _f32p, _i32p, _i32p, C.c_float, C.c_float,
@@ -194,29 +194,56 @@ class ConfigResult:
     virial: float
     escale: np.ndarray | None = None   # 4 eps sum_j (s^12 + s^6)        (FP64)
     fscale: np.ndarray | None = None   # 24 eps sum_j (2 s^12 + s^6) / r (FP64)
+    nnb: np.ndarray | None = None      # interacting neighbours per particle
 
-    def force_errors(self, f) -> dict:
-        """Errors of a float force array (sorted order) against the FP64 result."""
+    def representable(self):
+        """Particles whose FP64 energy, force and conditioning scales fit in float32 (FLT_MAX 3.4e38)."""
+        lim = 1e38
+        ok = np.abs(self.e64) < lim
+        ok &= np.all(np.abs(self.f64) < lim, axis=1)
+        if self.fscale is not None:
+            ok &= (self.fscale < lim) & (self.escale < lim)
+        return ok
+
+    def scaled_tolerance(self, base: float = 1e-5):
+        """Per-particle tolerance for float sums of m_i terms: max(base, 16 u sqrt(m_i)), u = 2^-24."""
+        m = self.nnb if self.nnb is not None else np.ones(len(self.e64))
+        return np.maximum(base, 16.0 * 2.0 ** -24 * np.sqrt(np.maximum(m, 1)))
+
+    def force_errors(self, f, tol_base: float = 1e-5) -> dict:
+        """Errors of a float force array (sorted order) against the FP64 result,
+        over the particles whose FP64 results are representable in float."""
         f = np.asarray(f, np.float64).reshape(-1, 3)
-        d = np.linalg.norm(f - self.f64, axis=1)
-        fn = np.linalg.norm(self.f64, axis=1)
+        ok = self.representable()
+        d = np.linalg.norm(f - self.f64, axis=1)[ok]
+        f64 = self.f64[ok]
+        fn = np.linalg.norm(f64, axis=1)
         nz = fn > 0
         rel = d[nz] / fn[nz]
-        out = {"normwise": float(np.linalg.norm(f - self.f64) / max(np.linalg.norm(self.f64), 1e-300)),
+        out = {"normwise": float(np.linalg.norm(f[ok] - f64) / max(np.linalg.norm(f64), 1e-300)),
                "max_rel": float(rel.max()) if rel.size else 0.0,
-               "p99_rel": float(np.percentile(rel, 99)) if rel.size else 0.0}
+               "p99_rel": float(np.percentile(rel, 99)) if rel.size else 0.0,
+               "excluded": int((~ok).sum())}
         if self.fscale is not None:
-            sc = self.fscale > 0
-            out["max_scaled"] = float((d[sc] / self.fscale[sc]).max()) if sc.any() else 0.0
+            sc = self.fscale[ok] > 0
+            ratio = d[sc] / self.fscale[ok][sc]
+            out["max_scaled"] = float(ratio.max()) if sc.any() else 0.0
+            out["max_scaled_over_tol"] = float((ratio / self.scaled_tolerance(tol_base)[ok][sc]).max()) \
+                if sc.any() else 0.0
         return out
 
-    def energy_errors(self, e) -> dict:
+    def energy_errors(self, e, tol_base: float = 1e-5) -> dict:
         e = np.asarray(e, np.float64)
-        d = np.abs(e - self.e64)
-        out = {"total_rel": float(abs(0.5 * e.sum() - self.etot) / max(abs(self.etot), 1e-300))}
+        ok = self.representable()
+        d = np.abs(e - self.e64)[ok]
+        out = {"total_rel": float(abs(0.5 * e.sum() - self.etot) / max(abs(self.etot), 1e-300)),
+               "excluded": int((~ok).sum())}
         if self.escale is not None:
-            sc = self.escale > 0
-            out["max_scaled"] = float((d[sc] / self.escale[sc]).max()) if sc.any() else 0.0
+            sc = self.escale[ok] > 0
+            ratio = d[sc] / self.escale[ok][sc]
+            out["max_scaled"] = float(ratio.max()) if sc.any() else 0.0
+            out["max_scaled_over_tol"] = float((ratio / self.scaled_tolerance(tol_base)[ok][sc]).max()) \
+                if sc.any() else 0.0
         return out
 
 
@@ -231,13 +258,14 @@ def config_forces(g: Grid, b: Binned, rc: float, eps: float = 1.0, sigma: float 
     f64 = np.empty((n, 3), np.float64) if want64 else None
     es = np.empty(n, np.float64) if want64 else None
     fs = np.empty(n, np.float64) if want64 else None
+    nnb = np.empty(n, np.int32)
     pairs = C.c_uint64(0)
     etot = C.c_double(0)
     vir = C.c_double(0)
     lib().ljo_config_forces(C.byref(g), n, b.sx, b.sy, b.sz, b.cell_sorted, b.offsets, rc, eps, sigma,
                             _ptr(e32), _ptr(f32), _ptr(e64), _ptr(f64), C.byref(pairs), C.byref(etot),
-                            C.byref(vir), _ptr(es), _ptr(fs))
-    return ConfigResult(e32, f32, e64, f64, int(pairs.value), float(etot.value), float(vir.value), es, fs)
+                            C.byref(vir), _ptr(es), _ptr(fs), _ptr(nnb))
+    return ConfigResult(e32, f32, e64, f64, int(pairs.value), float(etot.value), float(vir.value), es, fs, nnb)
 
 
 def config_forces_f32_range(g: Grid, b: Binned, k0: int, k1: int, rc: float, eps: float, sigma: float,

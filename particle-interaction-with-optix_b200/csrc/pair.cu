@@ -38,6 +38,7 @@ struct PairParams {
     float sig2;    // sigma^2
     float e4;      // 4 eps
     float e24;     // 24 eps
+    float fscale;  // -24 eps / sigma^2: converts the accumulated sum of t * s2 * d into a force
     float slack;   // absolute rounding slack for cell planes and window ends
 };
 
@@ -226,7 +227,8 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairPar
                     ea += s12 - s6;
                     const float t = fmaf(2.0f, s12, -s6);
                     wa += t;
-                    const float fs = ir2 * t;
+                    // force in units of 24 eps / sigma^2: t * s2 stays finite where t * ir2 would overflow
+                    const float fs = t * s2;
                     fx = fmaf(fs, dx, fx);
                     fy = fmaf(fs, dy, fy);
                     fz = fmaf(fs, dz, fz);
@@ -237,9 +239,9 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairPar
     done:
         if (energy) energy[k] = pp.e4 * ea;
         if (force) {
-            force[3 * (size_t)k + 0] = -pp.e24 * fx;
-            force[3 * (size_t)k + 1] = -pp.e24 * fy;
-            force[3 * (size_t)k + 2] = -pp.e24 * fz;
+            force[3 * (size_t)k + 0] = pp.fscale * fx;
+            force[3 * (size_t)k + 1] = pp.fscale * fy;
+            force[3 * (size_t)k + 2] = pp.fscale * fz;
         }
     }
     reduce_totals(0.5 * (double)pp.e4 * (double)ea, 0.5 * (double)pp.e24 * (double)wa, (unsigned long long)np, part,
@@ -310,6 +312,7 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
     pp.sig2 = prm->sigma * prm->sigma;
     pp.e4 = 4.0f * prm->epsilon;
     pp.e24 = 24.0f * prm->epsilon;
+    pp.fscale = -pp.e24 / pp.sig2;
     pp.slack = grid_slack(*g);
     unsigned* counter = static_cast<unsigned*>(ctx->red);
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
@@ -344,7 +347,7 @@ extern "C" lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* 
     if (!ctx || !g || !p || n < 0) return LJ_EINVAL;
     if (n > 0 && (!sorted_xyzi || !sorted_cell || !offsets)) return LJ_EINVAL;
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
-    if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width)) return LJ_EINVAL;
+    if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;
     if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
     if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
     return launch_pair_config(ctx, g, p, n, sorted_xyzi, sorted_cell, offsets, order, energy, force, totals);

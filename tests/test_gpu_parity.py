@@ -11,7 +11,10 @@ import ljoracle as O
 pytestmark = pytest.mark.gpu
 
 # FP32 pair math against the FP64 oracle: error relative to each particle's
-# conditioning scale (sum of the pair terms' magnitudes before cancellation).
+# conditioning scale (sum of the pair terms' magnitudes before cancellation),
+# at most max(1e-5, 16 u sqrt(m)) for a particle with m interacting neighbours
+# (u = 2^-24: float summation error grows like u sqrt(m)).  Particles whose
+# FP64 energy or force exceeds the float range are not compared.
 FORCE_SCALED_TOL = 1e-5
 ENERGY_SCALED_TOL = 1e-5
 FORCE_NORMWISE_TOL = 1e-5     # ||F - F64|| / ||F64|| over all particles
@@ -255,12 +258,12 @@ def test_config_forces(torch_cuda, ctx, name, order):
     assert t["pairs"] == ref.pairs
     e = np_(energy)[:n]
     f = np_(force)[:n]
-    fe = ref.force_errors(f)
-    ee = ref.energy_errors(e)
-    assert fe["max_scaled"] <= FORCE_SCALED_TOL, fe
+    fe = ref.force_errors(f, FORCE_SCALED_TOL)
+    ee = ref.energy_errors(e, ENERGY_SCALED_TOL)
+    assert fe["max_scaled_over_tol"] <= 1.0, fe
     assert fe["normwise"] <= FORCE_NORMWISE_TOL, fe
-    assert ee["max_scaled"] <= ENERGY_SCALED_TOL, ee
-    if ref.pairs:
+    assert ee["max_scaled_over_tol"] <= 1.0, ee
+    if ref.pairs and fe["excluded"] == 0:
         assert abs(t["energy"] - ref.etot) <= TOTAL_ENERGY_TOL * abs(ref.etot), (t["energy"], ref.etot)
         assert abs(t["virial"] - ref.virial) <= TOTAL_ENERGY_TOL * abs(ref.virial) + 1e-300
         assert abs(t["energy"] - 0.5 * e.astype(np.float64).sum()) <= 1e-12 * abs(ref.etot) + 1e-300
