@@ -301,7 +301,7 @@ def run_ours(args, cfg):
     algo_flops = FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs
     pair_ms = float(t_pair.mean())
     achieved = algo_flops / (pair_ms * 1e-3) / 1e12
-    traffic = read_traffic("k_pair_config", cfg["workload"])
+    traffic = read_traffic("k_pair_tiled", cfg["workload"])
 
     e2e = None
     if not args.no_e2e:
@@ -331,13 +331,13 @@ def run_ours(args, cfg):
             "pairs_per_step": pairs, "candidate_pairs_per_step": c_ref,
             "candidate_pairs_per_s": c_ref * ws / (t_max_ms * 1e-3),
             "particles_per_s": n * ws / (t_max_ms * 1e-3),
-            "roofline": {"kernel": "k_pair_config", "bound": "fp32", "achieved": achieved, "peak": peak_tflops,
+            "roofline": {"kernel": "k_pair_tiled", "bound": "fp32", "achieved": achieved, "peak": peak_tflops,
                          "unit": "TFLOP/s", "frac": achieved / peak_tflops, "traffic": traffic,
                          "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 flop x {sm_mhz:.0f} MHz (median sampled "
                                         "SM clock; MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
                          "algorithmic_flops": algo_flops},
             "e2e": e2e,
-            "gpu_launches": 6 * K,
+            "gpu_launches": 7 * K,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         }
         if cpu:

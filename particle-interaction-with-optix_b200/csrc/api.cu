@@ -107,6 +107,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->tmp4);
     cudaFree(c->large_cells);
     cudaFree(c->red);
+    cudaFree(c->tiles);
     cudaFree(c->e2e);
     delete c;
     return LJ_OK;

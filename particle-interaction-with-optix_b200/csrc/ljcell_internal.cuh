@@ -96,6 +96,8 @@ struct lj_ctx {
     void* red;                   // reduction partials + counter
     size_t red_bytes;
     unsigned long long* d_cand;  // candidate-count accumulator
+    void* tiles;                 // tile counter, tile count and cell-block tiles of the pair kernel
+    size_t tiles_bytes;
     // end-to-end buffers (lj_simulate_host)
     void* e2e;
     size_t e2e_bytes;
