@@ -194,6 +194,25 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
                      const int* sorted_cell, const int* offsets, lj_order order, float* energy, float* force,
                      lj_totals* totals);
 
+/* ------------------------------------------------------------- tuning
+ * Implementation choices of the context (no counterpart in the reference,
+ * whose launch shape is fixed at 128 threads per particle, cudaLJ.cu:519-520).
+ * Results do not depend on them except in the last bits of floating-point
+ * sums.  pair_kernel, for particles binned with LJ_ORDER_X:
+ *   0 = default,
+ *   1 = direct: one thread per target, neighbours through L1,
+ *   2 = direct with compaction: interacting neighbours queued per lane and
+ *       the pair law evaluated only for them,
+ *   3 = tiled: cell-block tiles staged in shared memory by TMA bulk copies
+ *       (totals summed in tile order: not bitwise reproducible run to run). */
+typedef struct {
+    int pair_kernel;
+    int reserved[7];
+} lj_tuning;
+
+LJ_API lj_status lj_set_tuning(lj_ctx* ctx, const lj_tuning* t);
+LJ_API lj_status lj_get_tuning(lj_ctx* ctx, lj_tuning* t);
+
 /* ------------------------------------------------------------- end to end
  * One call with HOST buffers, the shape of executeSimulation's step
  * (cudaLJ.cu:613-653) without the generation: copies positions to the device,

@@ -119,6 +119,18 @@ extern "C" lj_status lj_set_stream(lj_ctx* c, void* stream) {
     return LJ_OK;
 }
 
+extern "C" lj_status lj_set_tuning(lj_ctx* c, const lj_tuning* t) {
+    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 3) return LJ_EINVAL;
+    c->tuning = *t;
+    return LJ_OK;
+}
+
+extern "C" lj_status lj_get_tuning(lj_ctx* c, lj_tuning* t) {
+    if (!c || !t) return LJ_EINVAL;
+    *t = c->tuning;
+    return LJ_OK;
+}
+
 extern "C" lj_status lj_sync(lj_ctx* c) {
     if (!c) return LJ_EINVAL;
     DeviceScope scope(c->device);

@@ -96,6 +96,7 @@ struct lj_ctx {
     void* red;                   // reduction partials + counter
     size_t red_bytes;
     unsigned long long* d_cand;  // candidate-count accumulator
+    lj_tuning tuning;            // implementation choices (lj_set_tuning)
     void* tiles;                 // tile counter, tile count and cell-block tiles of the pair kernel
     size_t tiles_bytes;
     // end-to-end buffers (lj_simulate_host)

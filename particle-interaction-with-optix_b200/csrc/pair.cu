@@ -188,7 +188,13 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
     pp.e24 = 24.0f * prm->epsilon;
     pp.fscale = -pp.e24 / pp.sig2;
     pp.slack = grid_slack(*g);
-    if (order == LJ_ORDER_X) return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
+    if (order == LJ_ORDER_X) {
+        switch (ctx->tuning.pair_kernel) {
+            case 3: return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
+            case 2: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals);
+            default: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals);
+        }
+    }
     const int blocks = (n + kPairThreads - 1) / kPairThreads;
     const size_t need = 256 + (size_t)blocks * sizeof(Partial);
     if (need > ctx->red_bytes) {

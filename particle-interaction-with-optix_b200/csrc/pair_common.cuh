@@ -129,6 +129,9 @@ __device__ void reduce_totals(double e, double w, unsigned long long np, Partial
 
 
 float grid_slack(const lj_grid& g);
+lj_status launch_pair_direct(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
+                             const int* cs, const int* off, bool compact, float* energy, float* force,
+                             lj_totals* totals);
 lj_status launch_pair_tiled(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                             const int* off, float* energy, float* force, lj_totals* totals);
 

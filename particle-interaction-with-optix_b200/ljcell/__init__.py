@@ -56,6 +56,12 @@ class Particles(C.Structure):
                 ("index", C.c_void_p), ("nbParticles", C.c_int)]
 
 
+class Tuning(C.Structure):
+    """lj_tuning: implementation choices (pair_kernel 0 default, 1 direct, 2 direct+compaction, 3 tiled)."""
+
+    _fields_ = [("pair_kernel", C.c_int), ("reserved", C.c_int * 7)]
+
+
 class LJError(RuntimeError):
     def __init__(self, status: int, where: str):
         super().__init__(f"{where}: {status_str(status)} (status {status})")
@@ -87,6 +93,8 @@ def _load() -> C.CDLL:
         "lj_count_candidates": (i32, [vp, C.POINTER(Grid), vp, vp]),
         "lj_compute_compat": (i32, [vp, C.POINTER(Grid), i32, vp, vp, vp, vp]),
         "lj_compute": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, i32, vp, vp, vp]),
+        "lj_set_tuning": (i32, [vp, C.POINTER(Tuning)]),
+        "lj_get_tuning": (i32, [vp, C.POINTER(Tuning)]),
         "lj_simulate_host": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
                                    C.POINTER(Totals)]),
     }
@@ -101,7 +109,7 @@ _lib = _load()
 ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj_set_stream", "lj_sync",
                "lj_generate_uniform", "lj_generate_sphere", "lj_grid_from_box", "lj_grid_compat",
                "lj_count_cells", "lj_exclusive_scan", "lj_cell_descriptors", "lj_bin", "lj_count_candidates",
-               "lj_compute_compat", "lj_compute", "lj_simulate_host")
+               "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_simulate_host")
 
 
 def lib() -> C.CDLL:
@@ -196,6 +204,16 @@ class Context:
 
     def sync(self):
         _check(_lib.lj_sync(self._h), "lj_sync")
+
+    def set_tuning(self, pair_kernel: int = 0):
+        t = Tuning()
+        t.pair_kernel = pair_kernel
+        _check(_lib.lj_set_tuning(self._h, C.byref(t)), "lj_set_tuning")
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        _check(_lib.lj_get_tuning(self._h, C.byref(t)), "lj_get_tuning")
+        return {"pair_kernel": t.pair_kernel}
 
     # ------------------------------------------------------------ generation
     def _gen_out(self, n, want_soa, want_aos):

@@ -241,12 +241,17 @@ def test_compat_energy(torch_cuda, ctx, name, order):
 
 
 # ------------------------------------------------------------------ config law
-@pytest.mark.parametrize("order", [0, 1])
+# (order, pair kernel): LJ_ORDER_INDEX has one kernel; LJ_ORDER_X has direct, direct with compaction, tiled
+VARIANTS = [(0, 0), (1, 1), (1, 2), (1, 3)]
+
+
+@pytest.mark.parametrize("order,kernel", VARIANTS, ids=[f"order{o}-k{k}" for o, k in VARIANTS])
 @pytest.mark.parametrize("name", ["uniform_c1", "uniform_dense", "shell", "clustered", "outside_and_faces",
                                   "tiny2", "tiny33"])
-def test_config_forces(torch_cuda, ctx, name, order):
+def test_config_forces(torch_cuda, ctx, name, order, kernel):
     import ljcell
 
+    ctx.set_tuning(kernel)
     (x, y, z), g, og, b, ob, rc = bin_both(torch_cuda, ctx, name, order)
     # the cluster packs 5000 particles into 1e-6 volume: a small sigma keeps s^12 inside float range
     p = ljcell.params(rc, sigma=rc / 500 if name == "clustered" else None)
@@ -263,6 +268,7 @@ def test_config_forces(torch_cuda, ctx, name, order):
     assert fe["max_scaled_over_tol"] <= 1.0, fe
     assert fe["normwise"] <= FORCE_NORMWISE_TOL, fe
     assert ee["max_scaled_over_tol"] <= 1.0, ee
+    ctx.set_tuning(0)
     if ref.pairs and fe["excluded"] == 0:
         assert abs(t["energy"] - ref.etot) <= TOTAL_ENERGY_TOL * abs(ref.etot), (t["energy"], ref.etot)
         assert abs(t["virial"] - ref.virial) <= TOTAL_ENERGY_TOL * abs(ref.virial) + 1e-300
@@ -288,10 +294,12 @@ def test_config_tiny_cutoff_pair_count(torch_cuda, ctx):
     assert ljcell.totals_from_tensor(tot)["pairs"] == ref.pairs
 
 
-def test_deterministic(torch_cuda, ctx):
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+def test_deterministic(torch_cuda, ctx, kernel):
     import ljcell
 
     torch = torch_cuda
+    ctx.set_tuning(kernel)
     (x, y, z), (lo, hi), rc = case_positions("uniform_c1")
     g = ljcell.grid_from_box(lo, hi, rc)
     outs = []
@@ -300,6 +308,7 @@ def test_deterministic(torch_cuda, ctx):
         e, f, tot = ctx.compute(g, ljcell.params(rc), b)
         ctx.sync()
         outs.append((np_(b.xyzi), np_(e), np_(f), np_(tot)))
+    ctx.set_tuning(0)
     for a, c in zip(*outs):
         assert np.array_equal(a.view(np.uint8), c.view(np.uint8))
 
