@@ -148,6 +148,27 @@ LJ_API lj_status lj_count_cells(lj_ctx* ctx, const lj_grid* g, int n, const floa
  * no per-call allocation, no host synchronisation.  Device pointers. */
 LJ_API lj_status lj_exclusive_scan(lj_ctx* ctx, const int* counts, long long ncells, int* offsets);
 
+/* Allocation-free exclusive scan (no counterpart in the reference).  For
+ * callers that cannot allocate device memory -- code inside a host that owns
+ * every byte of the device through its own pool, or code that must not pay
+ * the device-wide synchronisation cudaMalloc/cudaFree can cause -- and so
+ * cannot create an lj_ctx.  Same result as lj_exclusive_scan, computed by the
+ * same kernel; its look-back scratch is a fixed array inside the library
+ * (256 bytes + 8 bytes per 4096 cells, 128 KiB), which every GPU that loads
+ * the library holds until the process exits.
+ *   - ncells <= 67,108,864 (2^26); larger returns LJ_EUNSUPPORTED.
+ *   - No cudaMalloc / cudaFree and no allocating library call.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture begins.
+ *   - Every call uses the same array: calls that may overlap on the GPU
+ *     (different streams, no ordering between them) race and must not be
+ *     issued.  Each call clears the part it uses before the scan.
+ *   - Asynchronous on `stream` (a cudaStream_t, NULL = legacy default).  A
+ *     bounded look-back wait that gave up (never expected) sets
+ *     offsets[ncells] = -1 instead of the total. */
+LJ_API lj_status lj_exclusive_scan_noalloc(const int* counts, long long ncells, int* offsets, void* stream);
+
 /* Cell descriptors from offsets, replaces InitNewCells (cudaLJ.cu:428-439). */
 LJ_API lj_status lj_cell_descriptors(lj_ctx* ctx, const int* offsets, long long ncells, lj_cell_desc* cells);
 

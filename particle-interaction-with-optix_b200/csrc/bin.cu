@@ -13,6 +13,7 @@
 // and ComputeNbInteractions (cudaLJ.cu:255-297) -> k_candidates (per cell
 // instead of per particle).
 #include <climits>
+#include <mutex>
 
 #include "ljcell_internal.cuh"
 
@@ -578,5 +579,75 @@ extern "C" lj_status lj_count_candidates(lj_ctx* ctx, const lj_grid* g, const in
     if (s != LJ_OK) return s;
     if (cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), ctx->stream) != cudaSuccess) return LJ_ECUDA;
     k_candidates<<<grid_for(ctx, nc, 256), 256, 0, ctx->stream>>>(to_dev(*g), offsets, nc, d_count);
+    return last_launch_status();
+}
+
+// ---------------------------------------------------------------- allocation-free scan
+// Some callers cannot allocate device memory at all: code running under an
+// allocator that forbids cudaMalloc (a memory pool that owns the whole device,
+// a pre-sized plugin host) or code that must not stall other streams on the
+// implicit synchronisation that cudaMalloc / cudaFree can cause.  For them
+// lj_exclusive_scan_noalloc runs k_scan with its look-back scratch (tile
+// counter + one 64-bit state per 4096-cell tile) in this file-scope array
+// instead of a context's allocation.  Every GPU that loads the library holds
+// the array (kNoAllocScratchBytes) until the process exits.
+namespace ljc {
+
+constexpr long long kNoAllocMaxCells = 1LL << 26;  // 67,108,864 cells
+constexpr long long kNoAllocMaxTiles = kNoAllocMaxCells / kScanTile;
+constexpr size_t kNoAllocScratchBytes = 256 + (size_t)kNoAllocMaxTiles * sizeof(unsigned long long);
+
+// [0, 4): tile counter; [4, 8): status word; [256, ...): tile states.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_addr[kNoAllocMaxDevices];
+
+// Device address of the array on the current device, looked up once per device.
+static lj_status noalloc_scratch(void** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return LJ_ECUDA;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return LJ_ECUDA;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return LJ_OK;
+}
+
+// A look-back that gave up (kFlagTimeout in the array's status word) marks
+// the result invalid with offsets[n] = -1; a valid total is never negative.
+__global__ void k_noalloc_mark(const unsigned* status, int* offsets, long long n) {
+    if (*status) offsets[n] = -1;
+}
+
+}  // namespace ljc
+
+extern "C" lj_status lj_exclusive_scan_noalloc(const int* counts, long long ncells, int* offsets, void* stream) {
+    if (ncells < 0 || !offsets || (ncells > 0 && !counts)) return LJ_EINVAL;
+    if (ncells > kNoAllocMaxCells) return LJ_EUNSUPPORTED;
+    void* scratch = nullptr;
+    lj_status s = noalloc_scratch(&scratch);
+    if (s != LJ_OK) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (ncells == 0) return cudaMemsetAsync(offsets, 0, sizeof(int), st) == cudaSuccess ? LJ_OK : LJ_ECUDA;
+    const long long ntiles = (ncells + kScanTile - 1) / kScanTile;
+    // the counter, status and the states this call uses must start at zero; the array keeps the last call's values
+    const size_t used = 256 + (size_t)ntiles * sizeof(unsigned long long);
+    if (cudaMemsetAsync(scratch, 0, used, st) != cudaSuccess) return LJ_ECUDA;
+    unsigned* counter = static_cast<unsigned*>(scratch);
+    unsigned* status = counter + 1;
+    unsigned long long* states = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) + 256);
+    const int vec_ok = ((reinterpret_cast<uintptr_t>(counts) | reinterpret_cast<uintptr_t>(offsets)) & 15) == 0;
+    k_scan<<<(unsigned)ntiles, kScanThreads, 0, st>>>(counts, offsets, ncells, ntiles, states, counter, vec_ok,
+                                                     status);
+    if ((s = last_launch_status()) != LJ_OK) return s;
+    k_noalloc_mark<<<1, 1, 0, st>>>(status, offsets, ncells);
     return last_launch_status();
 }

@@ -88,6 +88,7 @@ def _load() -> C.CDLL:
         "lj_grid_compat": (i32, [f32, f32, C.POINTER(Grid)]),
         "lj_count_cells": (i32, [vp, C.POINTER(Grid), i32, vp, vp, vp, i32, vp]),
         "lj_exclusive_scan": (i32, [vp, vp, i64, vp]),
+        "lj_exclusive_scan_noalloc": (i32, [vp, i64, vp, vp]),
         "lj_cell_descriptors": (i32, [vp, vp, i64, vp]),
         "lj_bin": (i32, [vp, C.POINTER(Grid), i32, vp, vp, vp, i32, i32, vp, vp, vp, C.POINTER(Particles), vp, vp]),
         "lj_count_candidates": (i32, [vp, C.POINTER(Grid), vp, vp]),
@@ -108,7 +109,7 @@ def _load() -> C.CDLL:
 _lib = _load()
 ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj_set_stream", "lj_sync",
                "lj_generate_uniform", "lj_generate_sphere", "lj_grid_from_box", "lj_grid_compat",
-               "lj_count_cells", "lj_exclusive_scan", "lj_cell_descriptors", "lj_bin", "lj_count_candidates",
+               "lj_count_cells", "lj_exclusive_scan", "lj_exclusive_scan_noalloc", "lj_cell_descriptors", "lj_bin", "lj_count_candidates",
                "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_simulate_host")
 
 
@@ -144,6 +145,16 @@ def grid_compat(box_width: float, cutoff: float) -> Grid:
 def default_sigma(cutoff: float) -> float:
     """sigma = r_c / 2.5 evaluated in float32."""
     return float(np.float32(cutoff) / np.float32(2.5))
+
+
+def exclusive_scan_noalloc(counts, offsets, stream=None):
+    """lj_exclusive_scan_noalloc: the scan without a context or any device
+    allocation (scratch is a fixed array inside the library).  `counts` and
+    `offsets` are int32 CUDA tensors (offsets has counts.numel() + 1 entries)."""
+    s = None if stream is None else C.c_void_p(stream.cuda_stream)
+    _check(_lib.lj_exclusive_scan_noalloc(_ptr(counts), int(counts.numel()), _ptr(offsets), s),
+           "lj_exclusive_scan_noalloc")
+    return offsets
 
 
 def params(cutoff: float, epsilon: float = 1.0, sigma: float | None = None) -> Params:
