@@ -220,11 +220,13 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  * whose launch shape is fixed at 128 threads per particle, cudaLJ.cu:519-520).
  * Results do not depend on them except in the last bits of floating-point
  * sums.  pair_kernel, for particles binned with LJ_ORDER_X:
- *   0 = default,
- *   1 = direct: one thread per target, neighbours through L1,
- *   2 = direct with compaction: interacting neighbours queued per lane and
+ *   0 = default (1),
+ *   1 = direct: one thread per target, neighbours through L1, its windows
+ *       in shared memory,
+ *   2 = direct with the windows in registers,
+ *   3 = direct with compaction: interacting neighbours queued per lane and
  *       the pair law evaluated only for them,
- *   3 = tiled: cell-block tiles staged in shared memory by TMA bulk copies
+ *   4 = tiled: cell-block tiles staged in shared memory by TMA bulk copies
  *       (totals summed in tile order: not bitwise reproducible run to run). */
 typedef struct {
     int pair_kernel;

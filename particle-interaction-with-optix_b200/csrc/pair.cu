@@ -33,91 +33,16 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairPar
                                                               Partial* part, unsigned* counter, lj_totals* totals,
                                                               unsigned* status) {
     __shared__ int2 s_win[kMaxWin][kPairThreads];
-    const int tid = threadIdx.x;
-    const int k = blockIdx.x * kPairThreads + tid;
+    const int k = blockIdx.x * kPairThreads + threadIdx.x;
     float ea = 0.f, fx = 0.f, fy = 0.f, fz = 0.f, wa = 0.f;
     unsigned np = 0;
     if (k < n) {
-        const float4 pi = p[k];
         int c = cs[k];
-        const int ncell = g.gx * g.gy * g.gz;
-        if (c < 0 || c >= ncell) {
+        if (c < 0 || c >= g.gx * g.gy * g.gz) {
             atomicOr(status, kFlagRange);
             c = 0;
         }
-        int cx, cy, cz;
-        decode_cell(g, c, cx, cy, cz);
-        const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
-        const float slack =
-            pp.slack + 8.0f * FLT_EPSILON * fmaxf(fabsf(pi.x), fmaxf(fabsf(pi.y), fabsf(pi.z)));
-        int nw = 0;
-#pragma unroll
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int z = cz + dz;
-            if (z < 0 || z >= g.gz) continue;
-            float dzm = 0.f;
-            if (XWIN) {
-                if (dz < 0) dzm = pi.z - fmaf((float)cz, g.w, g.oz);
-                if (dz > 0) dzm = fmaf((float)(cz + 1), g.w, g.oz) - pi.z;
-                dzm = fmaxf(dzm - slack, 0.f);
-            }
-#pragma unroll
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int y = cy + dy;
-                if (y < 0 || y >= g.gy) continue;
-                const int rb = (z * g.gy + y) * g.gx;
-                int s = min(max(__ldg(&off[rb + xl]), 0), n);
-                int e = min(max(__ldg(&off[rb + xh + 1]), s), n);
-                if (XWIN) {
-                    float dym = 0.f;
-                    if (dy < 0) dym = pi.y - fmaf((float)cy, g.w, g.oy);
-                    if (dy > 0) dym = fmaf((float)(cy + 1), g.w, g.oy) - pi.y;
-                    dym = fmaxf(dym - slack, 0.f);
-                    const float d2 = fmaf(dym, dym, dzm * dzm);
-                    if (d2 >= pp.rc2w) continue;
-                    const float h = sqrtf(pp.rc2w - d2) + slack;
-                    s = lower_x(p, s, e, pi.x - h);
-                    e = upper_x(p, s, e, pi.x + h);
-                }
-                if (dz == 0 && dy == 0) {
-                    s_win[nw++][tid] = make_int2(s, k);
-                    s_win[nw++][tid] = make_int2(k + 1, e);
-                } else {
-                    s_win[nw++][tid] = make_int2(s, e);
-                }
-            }
-        }
-        int w = 0;
-        int2 cur = s_win[0][tid];
-        const float rc2 = pp.rc2, sig2 = pp.sig2;
-        while (true) {
-            while (cur.x >= cur.y) {
-                if (++w >= nw) goto done;
-                cur = s_win[w][tid];
-            }
-            {
-                const float4 q = __ldg(&p[cur.x]);
-                ++cur.x;
-                const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                if (r2 < rc2) {
-                    const float ir2 = rcp_approx(r2);
-                    const float s2 = sig2 * ir2;
-                    const float s6 = s2 * s2 * s2;
-                    const float s12 = s6 * s6;
-                    ea += s12 - s6;
-                    const float t = fmaf(2.0f, s12, -s6);
-                    wa += t;
-                    // force in units of 24 eps / sigma^2: t * s2 stays finite where t * ir2 would overflow
-                    const float fs = t * s2;
-                    fx = fmaf(fs, dx, fx);
-                    fy = fmaf(fs, dy, fy);
-                    fz = fmaf(fs, dz, fz);
-                    ++np;
-                }
-            }
-        }
-    done:
+        pair_target<XWIN, kPairThreads>(g, pp, p, off, n, k, c, s_win, ea, fx, fy, fz, wa, np);
         if (energy) energy[k] = pp.e4 * ea;
         if (force) {
             force[3 * (size_t)k + 0] = pp.fscale * fx;
@@ -125,8 +50,8 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairPar
             force[3 * (size_t)k + 2] = pp.fscale * fz;
         }
     }
-    reduce_totals<kPairThreads>(0.5 * (double)pp.e4 * (double)ea, 0.5 * (double)pp.e24 * (double)wa, (unsigned long long)np, part,
-                  counter, totals);
+    reduce_totals<kPairThreads>(0.5 * (double)pp.e4 * (double)ea, 0.5 * (double)pp.e24 * (double)wa,
+                                (unsigned long long)np, part, counter, totals);
 }
 
 __global__ void __launch_bounds__(kPairThreads) k_pair_compat(GridDev g, const float4* __restrict__ p,
@@ -190,9 +115,10 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
     pp.slack = grid_slack(*g);
     if (order == LJ_ORDER_X) {
         switch (ctx->tuning.pair_kernel) {
-            case 3: return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
-            case 2: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals);
-            default: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals);
+            case 4: return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
+            case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals);
+            case 2: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals);
+            default: break;  // 0 and 1: windows in shared memory (below)
         }
     }
     const int blocks = (n + kPairThreads - 1) / kPairThreads;

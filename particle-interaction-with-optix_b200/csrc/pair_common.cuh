@@ -128,6 +128,90 @@ __device__ void reduce_totals(double e, double w, unsigned long long np, Partial
 }
 
 
+// Per-target work of the truncated law: windows and walk.  `c` is the
+// target's cell in grid g, `off` the offsets of that grid (values are indices
+// into p), `n` bounds every index.  Shared by the single-system kernel and
+// the batched kernel so both produce the same per-target results.
+template <bool XWIN, int BLOCK>
+__device__ __forceinline__ void pair_target(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
+                                            const int* __restrict__ off, int n, int k, int c,
+                                            int2 (*s_win)[BLOCK], float& ea, float& fx, float& fy, float& fz,
+                                            float& wa, unsigned& np) {
+    const int tid = threadIdx.x;
+    const float4 pi = p[k];
+    int cx, cy, cz;
+    decode_cell(g, c, cx, cy, cz);
+    const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
+    const float slack = pp.slack + 8.0f * FLT_EPSILON * fmaxf(fabsf(pi.x), fmaxf(fabsf(pi.y), fabsf(pi.z)));
+    int nw = 0;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int z = cz + dz;
+        if (z < 0 || z >= g.gz) continue;
+        float dzm = 0.f;
+        if (XWIN) {
+            if (dz < 0) dzm = pi.z - fmaf((float)cz, g.w, g.oz);
+            if (dz > 0) dzm = fmaf((float)(cz + 1), g.w, g.oz) - pi.z;
+            dzm = fmaxf(dzm - slack, 0.f);
+        }
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            if (y < 0 || y >= g.gy) continue;
+            const int rb = (z * g.gy + y) * g.gx;
+            int s = min(max(__ldg(&off[rb + xl]), 0), n);
+            int e = min(max(__ldg(&off[rb + xh + 1]), s), n);
+            if (XWIN) {
+                float dym = 0.f;
+                if (dy < 0) dym = pi.y - fmaf((float)cy, g.w, g.oy);
+                if (dy > 0) dym = fmaf((float)(cy + 1), g.w, g.oy) - pi.y;
+                dym = fmaxf(dym - slack, 0.f);
+                const float d2 = fmaf(dym, dym, dzm * dzm);
+                if (d2 >= pp.rc2w) continue;
+                const float h = sqrtf(pp.rc2w - d2) + slack;
+                s = lower_x(p, s, e, pi.x - h);
+                e = upper_x(p, s, e, pi.x + h);
+            }
+            if (dz == 0 && dy == 0) {
+                s_win[nw++][tid] = make_int2(s, k);
+                s_win[nw++][tid] = make_int2(k + 1, e);
+            } else {
+                s_win[nw++][tid] = make_int2(s, e);
+            }
+        }
+    }
+    int w = 0;
+    int2 cur = s_win[0][tid];
+    const float rc2 = pp.rc2, sig2 = pp.sig2;
+    while (true) {
+        while (cur.x >= cur.y) {
+            if (++w >= nw) return;
+            cur = s_win[w][tid];
+        }
+        {
+            const float4 q = __ldg(&p[cur.x]);
+            ++cur.x;
+            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            if (r2 < rc2) {
+                const float ir2 = rcp_approx(r2);
+                const float s2 = sig2 * ir2;
+                const float s6 = s2 * s2 * s2;
+                const float s12 = s6 * s6;
+                ea += s12 - s6;
+                const float t = fmaf(2.0f, s12, -s6);
+                wa += t;
+                // force in units of 24 eps / sigma^2: t * s2 stays finite where t * ir2 would overflow
+                const float fs = t * s2;
+                fx = fmaf(fs, dx, fx);
+                fy = fmaf(fs, dy, fy);
+                fz = fmaf(fs, dz, fz);
+                ++np;
+            }
+        }
+    }
+}
+
 float grid_slack(const lj_grid& g);
 lj_status launch_pair_direct(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                              const int* cs, const int* off, bool compact, float* energy, float* force,

@@ -57,7 +57,8 @@ class Particles(C.Structure):
 
 
 class Tuning(C.Structure):
-    """lj_tuning: implementation choices (pair_kernel 0 default, 1 direct, 2 direct+compaction, 3 tiled)."""
+    """lj_tuning: implementation choices (pair_kernel 0 default, 1 direct with shared-memory windows,
+    2 direct with register windows, 3 direct with compaction, 4 tiled)."""
 
     _fields_ = [("pair_kernel", C.c_int), ("reserved", C.c_int * 7)]
 

@@ -241,8 +241,8 @@ def test_compat_energy(torch_cuda, ctx, name, order):
 
 
 # ------------------------------------------------------------------ config law
-# (order, pair kernel): LJ_ORDER_INDEX has one kernel; LJ_ORDER_X has direct, direct with compaction, tiled
-VARIANTS = [(0, 0), (1, 1), (1, 2), (1, 3)]
+# (order, pair kernel): LJ_ORDER_INDEX has one kernel; LJ_ORDER_X has four (see lj_tuning)
+VARIANTS = [(0, 0), (1, 1), (1, 2), (1, 3), (1, 4)]
 
 
 @pytest.mark.parametrize("order,kernel", VARIANTS, ids=[f"order{o}-k{k}" for o, k in VARIANTS])
@@ -294,7 +294,7 @@ def test_config_tiny_cutoff_pair_count(torch_cuda, ctx):
     assert ljcell.totals_from_tensor(tot)["pairs"] == ref.pairs
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [1, 2, 3])
 def test_deterministic(torch_cuda, ctx, kernel):
     import ljcell
 
