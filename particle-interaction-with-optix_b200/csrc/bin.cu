@@ -248,6 +248,7 @@ __device__ __forceinline__ void emit(const SortOut& o, long long slot, float4 r,
 }
 
 constexpr int kWarpSortMax = 2048;
+constexpr int kLargeCap = 4096;  // cells beyond the warp sort, per step
 
 // One warp per group of 32 consecutive cells.  Lanes read the group's offsets
 // (coalesced), write the CellDescriptor view, copy singleton cells directly,
@@ -502,19 +503,11 @@ extern "C" lj_status lj_cell_descriptors(lj_ctx* ctx, const int* offsets, long l
     return last_launch_status();
 }
 
-extern "C" lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x, const float* y, const float* z,
-                            int stride, lj_order order, int* counts, int* offsets, lj_cell_desc* cells,
-                            lj_particles* sorted, float* sorted_xyzi, int* sorted_cell) {
-    long long nc;
-    if (!ctx || n < 0 || stride < 1 || !counts || !offsets) return LJ_EINVAL;
-    if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
-    lj_status s = check_grid(g, &nc);
-    if (s != LJ_OK) return s;
-    if (n > 0 && (!x || !y || !z || !sorted_xyzi || !sorted_cell)) return LJ_EINVAL;
-    if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
-    const GridDev gd = to_dev(*g);
-    cudaStream_t st = ctx->stream;
-    // scratch: per-particle (cell, ticket) and the unsorted float4 copy
+namespace ljc {
+
+// Stage 1 of a cell-grid build: scratch for n particles, counts zeroed.
+lj_status bin_prepare(lj_ctx* ctx, int n, long long nc, int* counts) {
+    lj_status s;
     const size_t need = (size_t)(n > 0 ? n : 1);
     if (need > ctx->part_cap) {
         void* p1 = ctx->cell_ticket;
@@ -526,21 +519,25 @@ extern "C" lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x
         ctx->tmp4 = static_cast<float4*>(p2);
         ctx->part_cap = need;
     }
-    const int large_cap = 4096;
     if (!ctx->large_cells) {
         void* p = nullptr;
         size_t cap = 0;
-        if ((s = grow(&p, &cap, sizeof(int) * (1 + large_cap))) != LJ_OK) return s;
+        if ((s = grow(&p, &cap, sizeof(int) * (1 + kLargeCap))) != LJ_OK) return s;
         ctx->large_cells = static_cast<int*>(p);
-        ctx->large_cap = large_cap;
+        ctx->large_cap = kLargeCap;
     }
-    if (cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, st) != cudaSuccess) return LJ_ECUDA;
-    if (cudaMemsetAsync(ctx->large_cells, 0, sizeof(int), st) != cudaSuccess) return LJ_ECUDA;
-    if (n > 0) {
-        k_count<true><<<grid_for(ctx, n, 256), 256, 0, st>>>(gd, x, y, z, stride, n, counts, ctx->cell_ticket,
-                                                             ctx->d_status);
-        if ((s = last_launch_status()) != LJ_OK) return s;
-    }
+    if (cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    if (cudaMemsetAsync(ctx->large_cells, 0, sizeof(int), ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    return LJ_OK;
+}
+
+// Stages after a count kernel has filled counts and ctx->cell_ticket: scan,
+// scatter, within-cell sort (with the descriptor view and SoA outputs).
+lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const float* y, const float* z, int stride,
+                     lj_order order, int* counts, int* offsets, lj_cell_desc* cells, lj_particles* sorted,
+                     float* sorted_xyzi, int* sorted_cell) {
+    lj_status s;
+    cudaStream_t st = ctx->stream;
     if ((s = launch_scan(ctx, counts, nc, offsets)) != LJ_OK) return s;
     if (n > 0) {
         k_scatter<<<grid_for(ctx, n, 256), 256, 0, st>>>(x, y, z, stride, n, ctx->cell_ticket, offsets, ctx->tmp4,
@@ -557,18 +554,39 @@ extern "C" lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x
     const int sort_blocks = grid_for(ctx, (nc + 31) / 32, 8, 16);
     if (order == LJ_ORDER_X) {
         k_cell_sort<LJ_ORDER_X><<<sort_blocks, 256, 0, st>>>(ctx->tmp4, offsets, nc, n, so, cells, ctx->large_cells,
-                                                            large_cap, ctx->d_status);
+                                                            kLargeCap, ctx->d_status);
         if ((s = last_launch_status()) != LJ_OK) return s;
         k_large_sort<LJ_ORDER_X><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so, ctx->large_cells,
-                                                                 large_cap);
+                                                                 kLargeCap);
     } else {
         k_cell_sort<LJ_ORDER_INDEX><<<sort_blocks, 256, 0, st>>>(ctx->tmp4, offsets, nc, n, so, cells,
-                                                                ctx->large_cells, large_cap, ctx->d_status);
+                                                                ctx->large_cells, kLargeCap, ctx->d_status);
         if ((s = last_launch_status()) != LJ_OK) return s;
         k_large_sort<LJ_ORDER_INDEX><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so, ctx->large_cells,
-                                                                     large_cap);
+                                                                     kLargeCap);
     }
     return last_launch_status();
+}
+
+}  // namespace ljc
+
+extern "C" lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x, const float* y, const float* z,
+                            int stride, lj_order order, int* counts, int* offsets, lj_cell_desc* cells,
+                            lj_particles* sorted, float* sorted_xyzi, int* sorted_cell) {
+    long long nc;
+    if (!ctx || n < 0 || stride < 1 || !counts || !offsets) return LJ_EINVAL;
+    if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
+    lj_status s = check_grid(g, &nc);
+    if (s != LJ_OK) return s;
+    if (n > 0 && (!x || !y || !z || !sorted_xyzi || !sorted_cell)) return LJ_EINVAL;
+    if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
+    if ((s = bin_prepare(ctx, n, nc, counts)) != LJ_OK) return s;
+    if (n > 0) {
+        k_count<true><<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(to_dev(*g), x, y, z, stride, n, counts,
+                                                                      ctx->cell_ticket, ctx->d_status);
+        if ((s = last_launch_status()) != LJ_OK) return s;
+    }
+    return bin_finish(ctx, nc, n, x, y, z, stride, order, counts, offsets, cells, sorted, sorted_xyzi, sorted_cell);
 }
 
 extern "C" lj_status lj_count_candidates(lj_ctx* ctx, const lj_grid* g, const int* offsets,

@@ -108,4 +108,9 @@ namespace ljc {
 // Host helpers shared by the .cu files (defined in api.cu).
 lj_status grow(void** p, size_t* cap, size_t need);
 lj_status last_launch_status();
+// Cell-grid build stages (bin.cu), shared by lj_bin and the batched step.
+lj_status bin_prepare(lj_ctx* ctx, int n, long long nc, int* counts);
+lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const float* y, const float* z, int stride,
+                     lj_order order, int* counts, int* offsets, lj_cell_desc* cells, lj_particles* sorted,
+                     float* sorted_xyzi, int* sorted_cell);
 }  // namespace ljc
