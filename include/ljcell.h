@@ -236,6 +236,62 @@ typedef struct {
 LJ_API lj_status lj_set_tuning(lj_ctx* ctx, const lj_tuning* t);
 LJ_API lj_status lj_get_tuning(lj_ctx* ctx, lj_tuning* t);
 
+/* ------------------------------------------------------------- batched systems
+ * Many independent systems of uneven sizes and cutoffs evaluated as one step
+ * (no counterpart in the reference, which runs one system per
+ * executeSimulation call).  The systems' particles sit back to back in one
+ * SoA array: system s owns [first, first + n).  All systems are binned by one
+ * launch per stage over a shared cell numbering, and the pair kernel is
+ * persistent: its CTAs take (system, cell-block) tiles from a device work
+ * queue, largest first. */
+typedef struct {
+    float lo[3];        /* box covered by the system's grid */
+    float hi[3];
+    lj_params params;   /* truncated law of the system (cutoff, epsilon, sigma) */
+    int first;          /* first particle of the system in the batch arrays */
+    int n;              /* particle count */
+} lj_system;
+
+typedef struct {
+    float cell_multiple; /* cell width = cell_multiple * cutoff (>= 1; default 1) */
+    int threads;         /* CTA size of the batched pair kernel: 64, 128 or 256 (default 128) */
+    int per_thread;      /* targets per thread in a tile: 1 or 2 (default 1) */
+    int reserved[5];
+} lj_batch_config;
+
+typedef struct lj_batch lj_batch;
+
+/* Plans a batch: takes host copies of `systems`, allocates the device tables
+ * and the batch's working buffers.  cfg may be NULL (defaults). */
+LJ_API lj_status lj_batch_create(lj_ctx* ctx, int nsys, const lj_system* systems, const lj_batch_config* cfg,
+                                 lj_batch** out);
+LJ_API lj_status lj_batch_destroy(lj_batch* b);
+LJ_API lj_status lj_batch_get_config(const lj_batch* b, lj_batch_config* cfg);
+/* Grid of system s under the batch's current configuration. */
+LJ_API lj_status lj_batch_grid(const lj_batch* b, int s, lj_grid* g);
+
+/* One step for every system: binning (LJ_ORDER_X) and the truncated law.
+ * x, y, z: device, all systems back to back.  Outputs (device, each may be
+ * NULL), per system in its own range [first, first + n) and in that system's
+ * cell order: energy, force (3 floats per particle), index (the batch-wide
+ * index of each sorted particle); totals[nsys]: each system's lj_totals. */
+LJ_API lj_status lj_batch_run(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
+                              float* energy, float* force, int* index, lj_totals* totals);
+/* The same step captured once in a CUDA graph for a given set of pointers and
+ * replayed; ordered after earlier work on the context's stream. */
+LJ_API lj_status lj_batch_run_graph(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
+                                    float* energy, float* force, int* index, lj_totals* totals);
+/* The same results computed with one lj_bin + lj_compute per system: the
+ * per-system plain launches the batched step replaces. */
+LJ_API lj_status lj_batch_run_separate(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
+                                       float* energy, float* force, int* index, lj_totals* totals);
+/* Autotuner: times every combination of cell_multiple {1, 1.5, 2}, threads
+ * {64, 128, 256} and per_thread {1, 2} on these inputs (graph replays), keeps
+ * the fastest in the plan and returns it with its time per step in ms.
+ * Synchronises. */
+LJ_API lj_status lj_batch_autotune(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
+                                   lj_batch_config* best, float* best_ms);
+
 /* ------------------------------------------------------------- end to end
  * One call with HOST buffers, the shape of executeSimulation's step
  * (cudaLJ.cu:613-653) without the generation: copies positions to the device,

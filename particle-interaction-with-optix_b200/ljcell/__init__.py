@@ -63,6 +63,20 @@ class Tuning(C.Structure):
     _fields_ = [("pair_kernel", C.c_int), ("reserved", C.c_int * 7)]
 
 
+class System(C.Structure):
+    """lj_system: box, truncated-law parameters and particle range of one system of a batch."""
+
+    _fields_ = [("lo", C.c_float * 3), ("hi", C.c_float * 3), ("params", Params), ("first", C.c_int),
+                ("n", C.c_int)]
+
+
+class BatchConfig(C.Structure):
+    """lj_batch_config: cell-width multiple, CTA size and targets per thread of the batched step."""
+
+    _fields_ = [("cell_multiple", C.c_float), ("threads", C.c_int), ("per_thread", C.c_int),
+                ("reserved", C.c_int * 5)]
+
+
 class LJError(RuntimeError):
     def __init__(self, status: int, where: str):
         super().__init__(f"{where}: {status_str(status)} (status {status})")
@@ -97,6 +111,14 @@ def _load() -> C.CDLL:
         "lj_compute": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, i32, vp, vp, vp]),
         "lj_set_tuning": (i32, [vp, C.POINTER(Tuning)]),
         "lj_get_tuning": (i32, [vp, C.POINTER(Tuning)]),
+        "lj_batch_create": (i32, [vp, i32, C.POINTER(System), C.POINTER(BatchConfig), C.POINTER(vp)]),
+        "lj_batch_destroy": (i32, [vp]),
+        "lj_batch_get_config": (i32, [vp, C.POINTER(BatchConfig)]),
+        "lj_batch_grid": (i32, [vp, i32, C.POINTER(Grid)]),
+        "lj_batch_run": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "lj_batch_run_graph": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "lj_batch_run_separate": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "lj_batch_autotune": (i32, [vp, vp, vp, vp, vp, C.POINTER(BatchConfig), C.POINTER(C.c_float)]),
         "lj_simulate_host": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
                                    C.POINTER(Totals)]),
     }
@@ -111,7 +133,9 @@ _lib = _load()
 ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj_set_stream", "lj_sync",
                "lj_generate_uniform", "lj_generate_sphere", "lj_grid_from_box", "lj_grid_compat",
                "lj_count_cells", "lj_exclusive_scan", "lj_exclusive_scan_noalloc", "lj_cell_descriptors", "lj_bin", "lj_count_candidates",
-               "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_simulate_host")
+               "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_batch_create",
+               "lj_batch_destroy", "lj_batch_get_config", "lj_batch_grid", "lj_batch_run", "lj_batch_run_graph",
+               "lj_batch_run_separate", "lj_batch_autotune", "lj_simulate_host")
 
 
 def lib() -> C.CDLL:
@@ -352,3 +376,143 @@ def totals_from_tensor(tot) -> dict:
     e, w = np.frombuffer(raw[:16], np.float64)
     pairs = int(np.frombuffer(raw[16:24], np.uint64)[0])
     return {"energy": float(e), "virial": float(w), "pairs": pairs}
+
+
+def totals_from_array(tot) -> list:
+    """Decodes k lj_totals held in a (k, 4) float64 tensor."""
+    raw = np.ascontiguousarray(tot.detach().cpu().numpy()).view(np.uint8).reshape(-1, 32)
+    out = []
+    for r in raw:
+        e, w = np.frombuffer(r[:16].tobytes(), np.float64)
+        out.append({"energy": float(e), "virial": float(w), "pairs": int(np.frombuffer(r[16:24].tobytes(),
+                                                                                         np.uint64)[0])})
+    return out
+
+
+# ------------------------------------------------------------------ batched systems
+class _Drand48:
+    """POSIX drand48 stream (srand48 semantics) for host-side workload parameters."""
+
+    def __init__(self, seed: int):
+        self.x = ((seed & 0xFFFFFFFF) << 16) | 0x330E
+
+    def __call__(self) -> float:
+        self.x = (0x5DEECE66D * self.x + 0xB) & ((1 << 48) - 1)
+        return self.x / float(1 << 48)
+
+
+def batch_workload(nsys: int = 512, seed: int = 1234, n_min: int = 1000, n_max: int = 200_000,
+                   nb_min: float = 20.0, nb_max: float = 200.0, shell_fraction: float = 0.25) -> list:
+    """Uneven systems: N log-uniform in [n_min, n_max], a mean neighbour count
+    uniform in [nb_min, nb_max] fixing each cutoff, a share of sphere-surface
+    systems (unit sphere about (0.5, 0.5, 0.5), box [-0.5, 1.5]^3) assigned by
+    a seeded shuffle, the rest uniform in [0, 1)^3; sigma = cutoff / 2.5.
+    Parameters come from one drand48 stream seeded with `seed`; system s's
+    positions use seed + s."""
+    d = _Drand48(seed)
+    nshell = int(round(nsys * shell_fraction))
+    kinds = ["shell"] * nshell + ["uniform"] * (nsys - nshell)
+    for i in range(nsys - 1, 0, -1):  # Fisher-Yates
+        j = int(d() * (i + 1))
+        kinds[i], kinds[j] = kinds[j], kinds[i]
+    out = []
+    ln = np.log(n_max / n_min)
+    for s in range(nsys):
+        n = int(round(np.exp(d() * ln) * n_min))
+        nb = nb_min + (nb_max - nb_min) * d()
+        if kinds[s] == "uniform":
+            rc = float(np.float32((3.0 * nb / (4.0 * np.pi * n)) ** (1.0 / 3.0)))
+            lo, hi = (0.0, 0.0, 0.0), (1.0, 1.0, 1.0)
+        else:
+            rc = float(np.float32(2.0 * np.sqrt(nb / n)))
+            lo, hi = (-0.5, -0.5, -0.5), (1.5, 1.5, 1.5)
+        out.append({"kind": kinds[s], "n": n, "cutoff": rc, "lo": lo, "hi": hi, "seed": seed + s,
+                    "neighbours": nb})
+    return out
+
+
+class Batch:
+    """An lj_batch: many systems, back to back in one SoA array, run as one step."""
+
+    def __init__(self, ctx: Context, systems: list, cell_multiple: float = 1.0, threads: int = 128,
+                 per_thread: int = 1):
+        self.ctx = ctx
+        self.systems = systems
+        arr = (System * len(systems))()
+        first = 0
+        for s, d in enumerate(systems):
+            a = arr[s]
+            a.lo[:] = [float(v) for v in d["lo"]]
+            a.hi[:] = [float(v) for v in d["hi"]]
+            a.params = params(d["cutoff"], d.get("epsilon", 1.0), d.get("sigma"))
+            a.first = first
+            a.n = int(d["n"])
+            d["first"] = first
+            first += a.n
+        self.ntotal = first
+        cfg = BatchConfig(cell_multiple, threads, per_thread)
+        h = C.c_void_p()
+        _check(_lib.lj_batch_create(ctx.handle, len(systems), arr, C.byref(cfg), C.byref(h)), "lj_batch_create")
+        self._h = h
+        self._arr = arr
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lj_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def config(self) -> dict:
+        c = BatchConfig()
+        _check(_lib.lj_batch_get_config(self._h, C.byref(c)), "lj_batch_get_config")
+        return {"cell_multiple": c.cell_multiple, "threads": c.threads, "per_thread": c.per_thread}
+
+    def grid(self, s: int) -> Grid:
+        g = Grid()
+        _check(_lib.lj_batch_grid(self._h, s, C.byref(g)), "lj_batch_grid")
+        return g
+
+    def params(self, s: int) -> Params:
+        return self._arr[s].params
+
+    def generate(self):
+        """Device positions of every system (seeded drand48), back to back."""
+        t = self.ctx.torch
+        x, y, z = (t.empty(max(self.ntotal, 1), dtype=t.float32, device=self.ctx.device) for _ in range(3))
+        for d in self.systems:
+            f, n = d["first"], d["n"]
+            if n == 0:
+                continue
+            p = Particles(x.data_ptr() + 4 * f, y.data_ptr() + 4 * f, z.data_ptr() + 4 * f, None, None, n)
+            if d["kind"] == "uniform":
+                _check(_lib.lj_generate_uniform(self.ctx.handle, d["seed"], n, _f3(d["lo"]), _f3(d["hi"]),
+                                                C.byref(p), None), "lj_generate_uniform")
+            else:
+                _check(_lib.lj_generate_sphere(self.ctx.handle, d["seed"], n, _f3((0.5, 0.5, 0.5)), 1.0,
+                                               C.byref(p), None), "lj_generate_sphere")
+        return x, y, z
+
+    def alloc_outputs(self):
+        t = self.ctx.torch
+        n = max(self.ntotal, 1)
+        dev = self.ctx.device
+        return (t.empty(n, dtype=t.float32, device=dev), t.empty((n, 3), dtype=t.float32, device=dev),
+                t.empty(n, dtype=t.int32, device=dev), t.zeros((len(self.systems), 4), dtype=t.float64, device=dev))
+
+    def run(self, x, y, z, energy=None, force=None, index=None, totals=None, mode: str = "plain"):
+        fn = {"plain": _lib.lj_batch_run, "graph": _lib.lj_batch_run_graph,
+              "separate": _lib.lj_batch_run_separate}[mode]
+        _check(fn(self.ctx.handle, self._h, _ptr(x), _ptr(y), _ptr(z), _ptr(energy), _ptr(force), _ptr(index),
+                  _ptr(totals)), f"lj_batch_run ({mode})")
+
+    def autotune(self, x, y, z):
+        c = BatchConfig()
+        ms = C.c_float(0)
+        _check(_lib.lj_batch_autotune(self.ctx.handle, self._h, _ptr(x), _ptr(y), _ptr(z), C.byref(c),
+                                      C.byref(ms)), "lj_batch_autotune")
+        return {"cell_multiple": c.cell_multiple, "threads": c.threads, "per_thread": c.per_thread}, float(ms.value)
