@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other workloads (batched 512 systems, sphere shell, dense) reported beside the headline")
     return ap.parse_args()
 
 
@@ -301,7 +303,7 @@ def run_ours(args, cfg):
     algo_flops = FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs
     pair_ms = float(t_pair.mean())
     achieved = algo_flops / (pair_ms * 1e-3) / 1e12
-    traffic = read_traffic("k_pair_tiled", cfg["workload"])
+    traffic = read_traffic("k_pair_config", cfg["workload"])
 
     e2e = None
     if not args.no_e2e:
@@ -311,6 +313,9 @@ def run_ours(args, cfg):
 
     if rank == 0 and ws == 1 and not args.no_ref_gpu:
         ref_gpu = reference_gpu(cfg, x, y, z, ctx, g)
+    extras = None
+    if rank == 0 and ws == 1 and not args.no_extras:
+        extras = run_extras(ctx, dev, flush, peak_tflops)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = CpuBaseline(cfg, args.seed)
@@ -331,25 +336,131 @@ def run_ours(args, cfg):
             "pairs_per_step": pairs, "candidate_pairs_per_step": c_ref,
             "candidate_pairs_per_s": c_ref * ws / (t_max_ms * 1e-3),
             "particles_per_s": n * ws / (t_max_ms * 1e-3),
-            "roofline": {"kernel": "k_pair_tiled", "bound": "fp32", "achieved": achieved, "peak": peak_tflops,
+            "roofline": {"kernel": "k_pair_config", "bound": "fp32", "achieved": achieved, "peak": peak_tflops,
                          "unit": "TFLOP/s", "frac": achieved / peak_tflops, "traffic": traffic,
                          "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 flop x {sm_mhz:.0f} MHz (median sampled "
                                         "SM clock; MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
                          "algorithmic_flops": algo_flops},
             "e2e": e2e,
-            "gpu_launches": 7 * K,
+            "gpu_launches": 6 * K,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         }
         if cpu:
             line["cpu_baseline"] = cpu
         if ref_gpu:
             line["reference_gpu"] = ref_gpu
+        if extras:
+            line["workloads"] = extras
         print(json.dumps(line), flush=True)
     ctx.close()
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def time_events(fn, reps, flush=None):
+    """Mean device time (ms) of fn() over reps calls, L2 flushed before each (outside the events)."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for i in range(reps):
+        if flush is not None:
+            flush.fill_(i & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return float(np.mean(ts))
+
+
+def single_workload(ctx, cfg, seed, flush, peak_tflops, reps=10):
+    """Plain FP32 step on one more single-system workload: stage times, pairs/s,
+    FP32 roofline of the pair kernel and, for the sphere shell, the HBM figure of
+    the whole step (76 B per particle + 16 B per cell, algorithmic)."""
+    import torch
+    import ljcell
+
+    n, rc = cfg["n"], cfg["rc"]
+    g = ljcell.grid_from_box(cfg["lo"], cfg["hi"], rc)
+    p = ljcell.params(rc)
+    if cfg["dist"] == "uniform":
+        soa, _ = ctx.generate_uniform(seed, n, cfg["lo"], cfg["hi"])
+    else:
+        soa, _ = ctx.generate_sphere(seed, n, (0.5, 0.5, 0.5), 1.0)
+    b = ctx.alloc_binned(g, n, ljcell.ORDER_X)
+    e, f, tot = ctx.alloc_outputs(n)
+    cand = torch.zeros(1, dtype=torch.int64, device=ctx.device)
+    t_bin = time_events(lambda: ctx.bin(g, soa["x"], soa["y"], soa["z"], order=ljcell.ORDER_X, out=b), reps, flush)
+    t_pair = time_events(lambda: ctx.compute(g, p, b, e, f, tot), reps, flush)
+    ctx.count_candidates(g, b.offsets, cand)
+    ctx.sync()
+    pairs = ljcell.totals_from_tensor(tot)["pairs"]
+    c_ref = int(cand.item())
+    step = t_bin + t_pair
+    ach = (FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs) / (t_pair * 1e-3) / 1e12
+    out = {"workload": cfg["workload"], "n": n, "cells": g.ncells, "ms_per_step": step,
+           "stage_ms": {"bin": t_bin, "pair": t_pair}, "pairs_per_step": pairs, "pairs_per_s": pairs / (step * 1e-3),
+           "particles_per_s": n / (step * 1e-3),
+           "pair_kernel_fp32": {"achieved_tflops": ach, "frac": ach / peak_tflops}}
+    if cfg["dist"] == "sphere":
+        algo_bytes = 76 * n + 16 * g.ncells
+        out["step_hbm"] = {"algorithmic_bytes": algo_bytes, "achieved_gbs": algo_bytes / (step * 1e-3) / 1e9,
+                           "peak_gbs": hbm_peak(), "frac": algo_bytes / (step * 1e-3) / 1e9 / hbm_peak()}
+    del soa, b, e, f, tot
+    torch.cuda.empty_cache()
+    return out
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
+def batched_workload(ctx, flush, reps=10):
+    """512 uneven systems (log-uniform N in [1e3, 2e5], 25% sphere shells): the
+    batched step replayed as one CUDA graph after autotuning, against the same
+    results from 512 per-system plain launches."""
+    import torch
+    import ljcell
+
+    w = ljcell.batch_workload()
+    b = ljcell.Batch(ctx, w)
+    x, y, z = b.generate()
+    e, f, idx, tot = b.alloc_outputs()
+    ctx.sync()
+    t0 = time.perf_counter()
+    cfg, _ = b.autotune(x, y, z)
+    tune_s = time.perf_counter() - t0
+    t_graph = time_events(lambda: b.run(x, y, z, e, f, None, tot, mode="graph"), reps, flush)
+    pairs = sum(t["pairs"] for t in ljcell.totals_from_array(tot))
+    t_sep = time_events(lambda: b.run(x, y, z, e, f, None, tot, mode="separate"), max(3, reps // 3), flush)
+    pairs_sep = sum(t["pairs"] for t in ljcell.totals_from_array(tot))
+    ctx.sync()
+    out = {"workload": "512 systems, N log-uniform [1e3, 2e5], 25% sphere shells, 20-200 neighbours",
+           "particles": b.ntotal, "pairs_per_step": pairs, "autotuned": cfg, "autotune_s": tune_s,
+           "ms_per_step_batched_graph": t_graph, "ms_per_step_per_system_launches": t_sep,
+           "speedup_vs_per_system": t_sep / t_graph, "pairs_per_s": pairs / (t_graph * 1e-3),
+           "pairs_match": pairs == pairs_sep}
+    b.close()
+    del x, y, z, e, f, idx, tot
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_extras(ctx, dev, flush, peak_tflops):
+    out = {}
+    out["batched_c5"] = batched_workload(ctx, flush)
+    out["shell_c3"] = single_workload(ctx, CONFIGS["c3"], 1234, flush, peak_tflops)
+    out["dense_c4"] = single_workload(ctx, CONFIGS["c4"], 1234, flush, peak_tflops)
+    return out
 
 
 def run_e2e(ctx, g, p, x, y, z, n, K, ws, dev, total_pairs, pairs):
