@@ -40,6 +40,7 @@ sys.path.insert(0, os.path.join(ROOT, "particle-interaction-with-optix_b200"))
 METRIC = "LJ pairs/sec @10M particles, plain vs mixed-precision/batched at ≤1e-5 err"
 FLOP_CANDIDATE = 8
 FLOP_INTERACTING = 18
+KERNEL_NAMES = {1: "k_pair_config", 2: "k_pair_direct<false>", 3: "k_pair_direct<true>"}
 
 CONFIGS = {
     "c1": dict(workload="uniform 100k, rc=0.05", n=100_000, dist="uniform", lo=(0, 0, 0), hi=(1, 1, 1), rc=0.05),
@@ -267,6 +268,9 @@ def run_ours(args, cfg):
     for _ in range(max(args.warmup, 3)):
         step()
     ctx.sync()
+    pair_kernel, _ = ctx.autotune_compute(g, p, b)   # outside the timed region
+    step()
+    ctx.sync()
     ctx.count_candidates(g, b.offsets, cand)
     ctx.sync()
     c_ref = int(cand.item())
@@ -303,7 +307,8 @@ def run_ours(args, cfg):
     algo_flops = FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs
     pair_ms = float(t_pair.mean())
     achieved = algo_flops / (pair_ms * 1e-3) / 1e12
-    traffic = read_traffic("k_pair_config", cfg["workload"])
+    kname = KERNEL_NAMES[pair_kernel]
+    traffic = read_traffic(kname, cfg["workload"])
 
     e2e = None
     if not args.no_e2e:
@@ -330,13 +335,14 @@ def run_ours(args, cfg):
             "dtype": "f32", "data": "synthetic (seeded drand48, device generated)",
             "config": {"workload": cfg["workload"], "n_per_gpu": n, "cutoff": rc, "sigma": p.sigma,
                        "cells": g.ncells, "order": "x-sorted within cells", "mode": "plain fp32",
+                       "pair_kernel": f"{pair_kernel} ({kname}, chosen by lj_autotune_compute)",
                        "l2": "flushed between steps (256 MiB write), flush excluded from timing",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single gpu"},
             "stage_ms": {"bin": float(t_bin.mean()), "pair": pair_ms},
             "pairs_per_step": pairs, "candidate_pairs_per_step": c_ref,
             "candidate_pairs_per_s": c_ref * ws / (t_max_ms * 1e-3),
             "particles_per_s": n * ws / (t_max_ms * 1e-3),
-            "roofline": {"kernel": "k_pair_config", "bound": "fp32", "achieved": achieved, "peak": peak_tflops,
+            "roofline": {"kernel": kname, "bound": "fp32", "achieved": achieved, "peak": peak_tflops,
                          "unit": "TFLOP/s", "frac": achieved / peak_tflops, "traffic": traffic,
                          "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 flop x {sm_mhz:.0f} MHz (median sampled "
                                         "SM clock; MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
@@ -396,7 +402,10 @@ def single_workload(ctx, cfg, seed, flush, peak_tflops, reps=10):
     e, f, tot = ctx.alloc_outputs(n)
     cand = torch.zeros(1, dtype=torch.int64, device=ctx.device)
     t_bin = time_events(lambda: ctx.bin(g, soa["x"], soa["y"], soa["z"], order=ljcell.ORDER_X, out=b), reps, flush)
+    saved = ctx.get_tuning()["pair_kernel"]
+    kern, _ = ctx.autotune_compute(g, p, b)
     t_pair = time_events(lambda: ctx.compute(g, p, b, e, f, tot), reps, flush)
+    ctx.set_tuning(saved)
     ctx.count_candidates(g, b.offsets, cand)
     ctx.sync()
     pairs = ljcell.totals_from_tensor(tot)["pairs"]
@@ -406,7 +415,7 @@ def single_workload(ctx, cfg, seed, flush, peak_tflops, reps=10):
     out = {"workload": cfg["workload"], "n": n, "cells": g.ncells, "ms_per_step": step,
            "stage_ms": {"bin": t_bin, "pair": t_pair}, "pairs_per_step": pairs, "pairs_per_s": pairs / (step * 1e-3),
            "particles_per_s": n / (step * 1e-3),
-           "pair_kernel_fp32": {"achieved_tflops": ach, "frac": ach / peak_tflops}}
+           "pair_kernel_fp32": {"kernel": KERNEL_NAMES[kern], "achieved_tflops": ach, "frac": ach / peak_tflops}}
     if cfg["dist"] == "sphere":
         algo_bytes = 76 * n + 16 * g.ncells
         out["step_hbm"] = {"algorithmic_bytes": algo_bytes, "achieved_gbs": algo_bytes / (step * 1e-3) / 1e9,

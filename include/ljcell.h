@@ -220,7 +220,7 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  * whose launch shape is fixed at 128 threads per particle, cudaLJ.cu:519-520).
  * Results do not depend on them except in the last bits of floating-point
  * sums.  pair_kernel, for particles binned with LJ_ORDER_X:
- *   0 = default (1),
+ *   0 = default: 2 when the grid averages 32 or more particles per cell, else 1,
  *   1 = direct: one thread per target, neighbours through L1, its windows
  *       in shared memory,
  *   2 = direct with the windows in registers,
@@ -234,6 +234,12 @@ typedef struct {
 } lj_tuning;
 
 LJ_API lj_status lj_set_tuning(lj_ctx* ctx, const lj_tuning* t);
+/* Autotuner for one system: times the deterministic pair kernels (1-3) on
+ * these binned (LJ_ORDER_X) particles and keeps the fastest in the context's
+ * tuning.  Synchronises. */
+LJ_API lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,
+                                     const float* sorted_xyzi, const int* sorted_cell, const int* offsets,
+                                     int* best_kernel, float* best_ms);
 LJ_API lj_status lj_get_tuning(lj_ctx* ctx, lj_tuning* t);
 
 /* ------------------------------------------------------------- batched systems

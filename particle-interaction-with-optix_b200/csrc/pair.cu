@@ -25,6 +25,8 @@
 
 namespace ljc {
 
+constexpr double kDenseCell = 32.0;  // particles per cell above which the default is the register-window kernel
+
 template <bool XWIN>
 __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairParams pp, const float4* __restrict__ p,
                                                               const int* __restrict__ cs,
@@ -114,11 +116,18 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
     pp.fscale = -pp.e24 / pp.sig2;
     pp.slack = grid_slack(*g);
     if (order == LJ_ORDER_X) {
-        switch (ctx->tuning.pair_kernel) {
+        int kernel = ctx->tuning.pair_kernel;
+        if (kernel == 0) {
+            // default: dense grids (many particles per cell, long windows) run best with the windows in
+            // registers, sparse ones with the windows in shared memory (measured on B200)
+            const double per_cell = (double)n / ((double)g->dim[0] * g->dim[1] * g->dim[2]);
+            kernel = per_cell >= kDenseCell ? 2 : 1;
+        }
+        switch (kernel) {
             case 4: return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
             case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals);
             case 2: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals);
-            default: break;  // 0 and 1: windows in shared memory (below)
+            default: break;  // 1: windows in shared memory (below)
         }
     }
     const int blocks = (n + kPairThreads - 1) / kPairThreads;
@@ -165,4 +174,44 @@ extern "C" lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* 
     if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
     if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
     return launch_pair_config(ctx, g, p, n, sorted_xyzi, sorted_cell, offsets, order, energy, force, totals);
+}
+
+extern "C" lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,
+                                         const float* sorted_xyzi, const int* sorted_cell, const int* offsets,
+                                         int* best_kernel, float* best_ms) {
+    if (!ctx || !g || !p || n < 1 || !sorted_xyzi || !sorted_cell || !offsets) return LJ_EINVAL;
+    const lj_tuning saved = ctx->tuning;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return LJ_ECUDA;
+    int best = 1;
+    float bt = 3.4e38f;
+    lj_status st = LJ_OK;
+    for (int k = 1; k <= 3 && st == LJ_OK; ++k) {
+        ctx->tuning.pair_kernel = k;
+        float ms = 3.4e38f;
+        for (int r = 0; r < 3 && st == LJ_OK; ++r) {  // the first run warms up
+            float one = 0.f;
+            if (cudaEventRecord(e0, ctx->stream) != cudaSuccess) st = LJ_ECUDA;
+            if (st == LJ_OK)
+                st = lj_compute(ctx, g, p, n, sorted_xyzi, sorted_cell, offsets, LJ_ORDER_X, nullptr, nullptr,
+                                nullptr);
+            if (st == LJ_OK && (cudaEventRecord(e1, ctx->stream) != cudaSuccess ||
+                                cudaEventSynchronize(e1) != cudaSuccess ||
+                                cudaEventElapsedTime(&one, e0, e1) != cudaSuccess))
+                st = LJ_ECUDA;
+            if (r > 0 && one < ms) ms = one;
+        }
+        if (st == LJ_OK && ms < bt) {
+            bt = ms;
+            best = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->tuning = saved;
+    if (st != LJ_OK) return st;
+    ctx->tuning.pair_kernel = best;
+    if (best_kernel) *best_kernel = best;
+    if (best_ms) *best_ms = bt;
+    return lj_sync(ctx);
 }

@@ -111,6 +111,8 @@ def _load() -> C.CDLL:
         "lj_compute": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, i32, vp, vp, vp]),
         "lj_set_tuning": (i32, [vp, C.POINTER(Tuning)]),
         "lj_get_tuning": (i32, [vp, C.POINTER(Tuning)]),
+        "lj_autotune_compute": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, C.POINTER(i32),
+                                      C.POINTER(C.c_float)]),
         "lj_batch_create": (i32, [vp, i32, C.POINTER(System), C.POINTER(BatchConfig), C.POINTER(vp)]),
         "lj_batch_destroy": (i32, [vp]),
         "lj_batch_get_config": (i32, [vp, C.POINTER(BatchConfig)]),
@@ -133,7 +135,7 @@ _lib = _load()
 ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj_set_stream", "lj_sync",
                "lj_generate_uniform", "lj_generate_sphere", "lj_grid_from_box", "lj_grid_compat",
                "lj_count_cells", "lj_exclusive_scan", "lj_exclusive_scan_noalloc", "lj_cell_descriptors", "lj_bin", "lj_count_candidates",
-               "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_batch_create",
+               "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_autotune_compute", "lj_batch_create",
                "lj_batch_destroy", "lj_batch_get_config", "lj_batch_grid", "lj_batch_run", "lj_batch_run_graph",
                "lj_batch_run_separate", "lj_batch_autotune", "lj_simulate_host")
 
@@ -245,6 +247,14 @@ class Context:
         t = Tuning()
         t.pair_kernel = pair_kernel
         _check(_lib.lj_set_tuning(self._h, C.byref(t)), "lj_set_tuning")
+
+    def autotune_compute(self, g: Grid, p: Params, b: Binned):
+        """Times pair kernels 1-3 on these binned particles and keeps the fastest."""
+        k = C.c_int(0)
+        ms = C.c_float(0)
+        _check(_lib.lj_autotune_compute(self._h, C.byref(g), C.byref(p), b.n, _ptr(b.xyzi), _ptr(b.cell),
+                                        _ptr(b.offsets), C.byref(k), C.byref(ms)), "lj_autotune_compute")
+        return int(k.value), float(ms.value)
 
     def get_tuning(self) -> dict:
         t = Tuning()

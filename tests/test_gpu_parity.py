@@ -332,3 +332,16 @@ def test_simulate_host_matches_device_path(torch_cuda, ctx):
     np.testing.assert_array_equal(hf, np_(f)[:n])
     np.testing.assert_array_equal(hi_, np_(b.xyzi)[:n, 3].view(np.int32))
     assert tot.pairs == ljcell.totals_from_tensor(t2)["pairs"]
+
+
+def test_autotune_compute_picks_a_kernel_and_keeps_results(torch_cuda, ctx):
+    import ljcell
+
+    (x, y, z), g, og, b, ob, rc = bin_both(torch_cuda, ctx, "uniform_dense", 1)
+    p = ljcell.params(rc)
+    kern, ms = ctx.autotune_compute(g, p, b)
+    assert kern in (1, 2, 3) and ms > 0 and ctx.get_tuning()["pair_kernel"] == kern
+    _, _, tot = ctx.compute(g, p, b)
+    ctx.sync()
+    ctx.set_tuning(0)
+    assert ljcell.totals_from_tensor(tot)["pairs"] == O.config_forces(og, ob, rc).pairs
