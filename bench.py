@@ -464,8 +464,74 @@ def batched_workload(ctx, flush, reps=10):
     return out
 
 
+def mixed_workload(ctx, cfg, seed, flush, reps=10, sample=100_000):
+    """Mixed-precision form beside the plain FP32 form on the same binned
+    particles: device times of the pair stage (records packed once per step,
+    counted), and errors on `sample` targets against FP64 on the stored
+    positions (the arithmetic) and between stored and original positions (the
+    binary16 inputs)."""
+    import torch
+    import ljcell
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ljoracle as O
+
+    n, rc = cfg["n"], cfg["rc"]
+    g = ljcell.grid_from_box(cfg["lo"], cfg["hi"], rc)
+    p = ljcell.params(rc)
+    soa, _ = ctx.generate_uniform(seed, n, cfg["lo"], cfg["hi"])
+    b = ctx.bin(g, soa["x"], soa["y"], soa["z"], order=ljcell.ORDER_X)
+    e, f, tot = ctx.alloc_outputs(n)
+    rec = ctx.pack_mixed(g, b)
+    saved = ctx.get_tuning()["pair_kernel"]
+    kern, _ = ctx.autotune_compute(g, p, b)
+    t_plain = time_events(lambda: ctx.compute(g, p, b, e, f, tot), reps, flush)
+    plain_pairs = ljcell.totals_from_tensor(tot)["pairs"]
+    ctx.set_tuning(saved)
+
+    def mixed_step():
+        ctx.pack_mixed(g, b, rec)
+        ctx.compute_mixed(g, p, b, rec, e, f, tot)
+
+    t_pack = time_events(lambda: ctx.pack_mixed(g, b, rec), reps, flush)
+    t_mixed = time_events(mixed_step, reps, flush)
+    ctx.sync()
+    mixed_pairs = ljcell.totals_from_tensor(tot)["pairs"]
+    # errors on a sample of targets, from the GPU's own sorted arrays
+    xyzi = b.xyzi.cpu().numpy()[:n]
+    ob = O.Binned(None, b.offsets.cpu().numpy(), xyzi[:, 3].view(np.int32).copy(), b.cell.cpu().numpy()[:n].copy(),
+                  np.ascontiguousarray(xyzi[:, 0]), np.ascontiguousarray(xyzi[:, 1]), np.ascontiguousarray(xyzi[:, 2]))
+    og = O.grid_from_box(cfg["lo"], cfg["hi"], rc)
+    uy, uz = O.pack_mixed(og, ob)
+    k0, k1 = n // 2, n // 2 + min(sample, n // 2)
+    stored = O.mixed_forces(og, ob, uy, uz, rc, 1.0, p.sigma, k0, k1)
+    fe = stored.force_errors(f.cpu().numpy()[k0:k1])
+    ee = stored.energy_errors(e.cpu().numpy()[k0:k1])
+    # the same sample with unrounded offsets: the effect of storing them in binary16
+    cy = (ob.cell_sorted // og.dim[0]) % og.dim[1]
+    cz = ob.cell_sorted // (og.dim[0] * og.dim[1])
+    w = np.float32(rc)
+    uy32 = ((ob.sy - (cy.astype(np.float32) * w + np.float32(og.origin[1]))) / w).astype(np.float32)
+    uz32 = ((ob.sz - (cz.astype(np.float32) * w + np.float32(og.origin[2]))) / w).astype(np.float32)
+    orig = O.mixed_forces(og, ob, uy32, uz32, rc, 1.0, p.sigma, k0, k1)
+    ok = orig.representable() & stored.representable()
+    q_err = float(np.linalg.norm(stored.f64[ok] - orig.f64[ok]) / np.linalg.norm(orig.f64[ok]))
+    out = {"workload": cfg["workload"] + ", mixed precision", "ms_pair_plain": t_plain,
+           "plain_kernel": KERNEL_NAMES[kern], "ms_pack_mixed": t_pack, "ms_pack_and_pair_mixed": t_mixed,
+           "speedup_vs_plain": t_plain / t_mixed, "pairs_plain": plain_pairs, "pairs_mixed": mixed_pairs,
+           "sample_targets": k1 - k0,
+           "error_vs_fp64_stored_positions": {"force_normwise": fe["normwise"], "force_max_scaled": fe["max_scaled"],
+                                              "force_p99_rel": fe["p99_rel"],
+                                              "energy_max_scaled": ee["max_scaled"]},
+           "binary16_input_effect": {"force_normwise_stored_vs_unrounded": q_err}}
+    del soa, b, e, f, tot, rec
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_extras(ctx, dev, flush, peak_tflops):
     out = {}
+    out["mixed_c4"] = mixed_workload(ctx, CONFIGS["c4"], 1234, flush)
     out["batched_c5"] = batched_workload(ctx, flush)
     out["shell_c3"] = single_workload(ctx, CONFIGS["c3"], 1234, flush, peak_tflops)
     out["dense_c4"] = single_workload(ctx, CONFIGS["c4"], 1234, flush, peak_tflops)

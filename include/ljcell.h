@@ -298,6 +298,27 @@ LJ_API lj_status lj_batch_run_separate(lj_ctx* ctx, lj_batch* b, const float* x,
 LJ_API lj_status lj_batch_autotune(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
                                    lj_batch_config* best, float* best_ms);
 
+/* ------------------------------------------------------------- mixed precision
+ * The mixed-precision form of the truncated law (no counterpart in the
+ * reference).  Storage: one 8-byte record per sorted particle, FP32 x and the
+ * y, z offsets from the particle's cell origin in cell widths as binary16
+ * (stored position = (x, oy + (cy + uy) w, oz + (cz + uz) w)): half the bytes
+ * of the float4 layout per neighbour load.  Pair math in FP32 (cell units),
+ * each particle's energy and force summed per stencil window and the window
+ * sums added with compensation (TwoSum), totals reduced in FP64.  Results
+ * are those of the stored positions: binary16 rounds the y, z offsets to
+ * 2^-11 .. 2^-12 of a cell width, and the pair count follows the mixed
+ * distance test (d in cell units, r2 < (cutoff / w)^2), restated exactly by
+ * the oracle. */
+
+/* Records from binned particles (LJ_ORDER_X).  rec: 2n floats, 8-byte aligned. */
+LJ_API lj_status lj_pack_mixed(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi,
+                               const int* sorted_cell, float* rec);
+/* Energy, force (sorted order) and totals from the records; as lj_compute. */
+LJ_API lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* rec,
+                                  const int* sorted_cell, const int* offsets, float* energy, float* force,
+                                  lj_totals* totals);
+
 /* ------------------------------------------------------------- end to end
  * One call with HOST buffers, the shape of executeSimulation's step
  * (cudaLJ.cu:613-653) without the generation: copies positions to the device,

@@ -478,3 +478,93 @@ LJO_EXPORT uint64_t ljo_brute_force(int64_t n, const float* x, const float* y, c
     }
     return pairs;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Mixed-precision form (new; not in the reference).  Records: x in float,  */
+/* y and z as binary16 offsets from the particle's cell origin in cell       */
+/* widths: u = (y - fmaf(cy, w, oy)) / w rounded to binary16.  The distance  */
+/* test is the kernel's, in cell units: dx = (xj - xi) * (1/w),              */
+/* dy = uyj - (uyi - (cyj - cyi)), dz likewise, r2 = fmaf(dz, dz, fmaf(dy,   */
+/* dy, dx*dx)) < (rc*rc) * (1/w) * (1/w).  The FP64 law runs on the stored   */
+/* positions (x, oy + (cy + uy) w, oz + (cz + uz) w).                        */
+/* ------------------------------------------------------------------------ */
+LJO_EXPORT void ljo_pack_mixed(const ljo_grid* g, int64_t n, const float* sy, const float* sz, const int* cell_sorted,
+                               float* uy, float* uz) {
+    for (int64_t k = 0; k < n; ++k) {
+        int cx, cy, cz;
+        ljo_coords(g, cell_sorted[k], &cx, &cy, &cz);
+        const float py = fmaf((float)cy, g->width, g->origin[1]);
+        const float pz = fmaf((float)cz, g->width, g->origin[2]);
+        uy[k] = (float)(_Float16)((sy[k] - py) / g->width);
+        uz[k] = (float)(_Float16)((sz[k] - pz) / g->width);
+    }
+}
+
+LJO_EXPORT void ljo_mixed_forces(const ljo_grid* g, int64_t k0, int64_t k1, const float* sx, const float* uy,
+                                 const float* uz, const int* cell_sorted, const int* offsets, float rc, float eps,
+                                 float sigma, double* e64, double* f64, uint64_t* pairs_out, double* etot_out,
+                                 double* vir_out, double* escale64, double* fscale64, int* nnb) {
+    const int gx = g->dim[0], gy = g->dim[1], gz = g->dim[2];
+    const float w = g->width;
+    const float invw = 1.0f / w;
+    const float rc2u = rc * rc * invw * invw;
+    const double wd = w, sig2d = (double)sigma * (double)sigma;
+    uint64_t pairs = 0;
+    double etot = 0.0, vir = 0.0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : pairs, etot, vir)
+    for (int64_t k = k0; k < k1; ++k) {
+        int cx, cy, cz;
+        ljo_coords(g, cell_sorted[k], &cx, &cy, &cz);
+        double ed = 0, fxd = 0, fyd = 0, fzd = 0, wd2 = 0, esd = 0, fsd = 0;
+        uint64_t np = 0;
+        for (int z = cz > 0 ? cz - 1 : 0; z <= (cz + 1 < gz ? cz + 1 : gz - 1); ++z)
+            for (int y = cy > 0 ? cy - 1 : 0; y <= (cy + 1 < gy ? cy + 1 : gy - 1); ++y) {
+                const float ty = uy[k] - (float)(y - cy);
+                const float tz = uz[k] - (float)(z - cz);
+                for (int x = cx > 0 ? cx - 1 : 0; x <= (cx + 1 < gx ? cx + 1 : gx - 1); ++x) {
+                    const int64_t c = ((int64_t)z * gy + y) * gx + x;
+                    for (int j = offsets[c]; j < offsets[c + 1]; ++j) {
+                        if (j == k) continue;
+                        const float dx = (sx[j] - sx[k]) * invw;
+                        const float dy = uy[j] - ty;
+                        const float dz = uz[j] - tz;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        if (!(r2 < rc2u)) continue;
+                        ++np;
+                        /* stored positions in double */
+                        const double ddx = (double)sx[j] - (double)sx[k];
+                        const double ddy = ((double)(y - cy) + (double)uy[j] - (double)uy[k]) * wd;
+                        const double ddz = ((double)(z - cz) + (double)uz[j] - (double)uz[k]) * wd;
+                        const double rr2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                        const double ir2 = 1.0 / rr2;
+                        const double s2 = sig2d * ir2, s6 = s2 * s2 * s2, s12 = s6 * s6;
+                        ed += s12 - s6;
+                        const double t = 2.0 * s12 - s6;
+                        wd2 += t;
+                        const double fs = ir2 * t;
+                        fxd += fs * ddx;
+                        fyd += fs * ddy;
+                        fzd += fs * ddz;
+                        esd += s12 + s6;
+                        fsd += ir2 * (2.0 * s12 + s6) * sqrt(rr2);
+                    }
+                }
+            }
+        pairs += np;
+        const double e4 = 4.0 * (double)eps, e24 = 24.0 * (double)eps;
+        if (e64) e64[k] = e4 * ed;
+        if (f64) {
+            f64[3 * k + 0] = -e24 * fxd;
+            f64[3 * k + 1] = -e24 * fyd;
+            f64[3 * k + 2] = -e24 * fzd;
+        }
+        if (escale64) escale64[k] = e4 * esd;
+        if (fscale64) fscale64[k] = e24 * fsd;
+        if (nnb) nnb[k] = (int)np;
+        etot += 0.5 * e4 * ed;
+        vir += 0.5 * e24 * wd2;
+    }
+    if (pairs_out) *pairs_out = pairs;
+    if (etot_out) *etot_out = etot;
+    if (vir_out) *vir_out = vir;
+}

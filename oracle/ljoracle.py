@@ -70,6 +70,11 @@ def _load():
     lib.ljo_lj_compat_many.argtypes = [C.c_int64, _f32p, _f32p, _f32p]
     lib.ljo_brute_force.restype = C.c_uint64
     lib.ljo_brute_force.argtypes = [C.c_int64, _f32p, _f32p, _f32p, C.c_float, C.c_float, C.c_float, _f64p, _f64p]
+    lib.ljo_pack_mixed.argtypes = [C.POINTER(Grid), C.c_int64, _f32p, _f32p, _i32p, _f32p, _f32p]
+    lib.ljo_mixed_forces.argtypes = [
+        C.POINTER(Grid), C.c_int64, C.c_int64, _f32p, _f32p, _f32p, _i32p, _i32p, C.c_float, C.c_float, C.c_float,
+        C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p,
+        C.c_void_p, C.c_void_p]
     return lib
 
 
@@ -342,3 +347,36 @@ def ref_run(x, y, z, box_width: float, cutoff: float, reps: int = 1) -> RefRun:
         raise RuntimeError(f"reference harness failed rc={rc} cuda_error={err} line={line.value}")
     out.nbinter = int(nb.value)
     return out
+
+
+# --------------------------------------------------------------------- mixed precision
+def pack_mixed(g: Grid, b: Binned):
+    """binary16 y, z offsets (as float) of the sorted particles, as the GPU record pack."""
+    n = len(b.sx)
+    uy = np.empty(n, np.float32)
+    uz = np.empty(n, np.float32)
+    lib().ljo_pack_mixed(C.byref(g), n, b.sy, b.sz, b.cell_sorted, uy, uz)
+    return uy, uz
+
+
+def mixed_forces(g: Grid, b: Binned, uy, uz, rc: float, eps: float = 1.0, sigma: float | None = None,
+                 k0: int = 0, k1: int | None = None) -> ConfigResult:
+    """FP64 law on the stored (mixed) positions, targets [k0, k1), pairs chosen by the mixed test.
+    Arrays of the result cover [k0, k1)."""
+    n = len(b.sx)
+    k1 = n if k1 is None else k1
+    if sigma is None:
+        sigma = float(np.float32(rc) / np.float32(2.5))
+    e64 = np.zeros(n, np.float64)
+    f64 = np.zeros((n, 3), np.float64)
+    es = np.zeros(n, np.float64)
+    fs = np.zeros(n, np.float64)
+    nnb = np.zeros(n, np.int32)
+    pairs = C.c_uint64(0)
+    etot = C.c_double(0)
+    vir = C.c_double(0)
+    lib().ljo_mixed_forces(C.byref(g), k0, k1, b.sx, uy, uz, b.cell_sorted, b.offsets, rc, eps, sigma, _ptr(e64),
+                           _ptr(f64), C.byref(pairs), C.byref(etot), C.byref(vir), _ptr(es), _ptr(fs), _ptr(nnb))
+    sl = slice(k0, k1)
+    return ConfigResult(None, None, e64[sl], f64[sl], int(pairs.value), float(etot.value), float(vir.value), es[sl],
+                        fs[sl], nnb[sl])

@@ -1,0 +1,259 @@
+// pair_mixed.cu -- the mixed-precision form of the truncated-LJ pair kernel.
+//
+// Storage.  One 8-byte record per sorted particle: x in FP32, and y, z as
+// FP16 offsets from the particle's cell origin in units of the cell width
+// (u = (y - (oy + cy w)) / w, rounded to binary16).  Stored positions are
+// therefore (x, oy + (cy + uy) w, oz + (cz + uz) w): FP32 cell origin + FP16
+// cell-relative offset in y and z, x exact because every stencil row is
+// x-sorted and the window search runs on it.  A candidate load moves 8 bytes
+// instead of 16.
+//
+// Arithmetic.  FP32, in cell units: for the stencil row at cell offset
+// (dy, dz) the target's frame Ty = uy_i - dy, Tz = uz_i - dz is set once per
+// window, so a candidate costs dy = uy_j - Ty, dz = uz_j - Tz and
+// dx = (x_j - x_i) / w.  Test r2 < (rc / w)^2 (exactly restated by the oracle).
+//
+// Accumulation.  Per window a plain FP32 partial; at each window switch the
+// partial is added to the running (sum, compensation) pair with TwoSum
+// (Knuth), so each particle's energy and force are compensated sums of
+// window partials.  Totals (energy, virial, pairs) reduce in FP64 as in
+// pair.cu.
+#include <cuda_fp16.h>
+
+#include "pair_common.cuh"
+
+namespace ljc {
+
+struct MixParams {
+    float invw;    // 1 / cell width
+    float w;       // cell width
+    float rc2u;    // (cutoff / w)^2 as rc2 * invw * invw: the distance test
+    float rc2uw;   // rc2u * (1 + 1e-5): row-skip and window bound
+    float sig2u;   // (sigma / w)^2
+    float e4;      // 4 eps
+    float e24;     // 24 eps
+    float fscale;  // -24 eps w / sigma^2: force from the sum of t s2 d (cell units)
+    float slack;   // absolute slack of the x window (as pair.cu)
+};
+
+// Knuth TwoSum: s + c absorbs the rounding error of adding v.
+__device__ __forceinline__ void two_sum_add(float& s, float& c, float v) {
+    const float t = s + v;
+    const float bp = t - s;
+    const float err = (s - (t - bp)) + (v - bp);
+    s = t;
+    c += err;
+}
+
+__global__ void __launch_bounds__(256) k_pack_mixed(GridDev g, const float4* __restrict__ p,
+                                                    const int* __restrict__ cs, int n, float2* __restrict__ rec) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 q = p[k];
+        int cx, cy, cz;
+        int c = cs[k];
+        const int nc = g.gx * g.gy * g.gz;
+        c = c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+        decode_cell(g, c, cx, cy, cz);
+        const float uy = __fdiv_rn(__fsub_rn(q.y, fmaf((float)cy, g.w, g.oy)), g.w);
+        const float uz = __fdiv_rn(__fsub_rn(q.z, fmaf((float)cz, g.w, g.oz)), g.w);
+        const __half2 h = __floats2half2_rn(uy, uz);
+        rec[k] = make_float2(q.x, __uint_as_float(*reinterpret_cast<const unsigned*>(&h)));
+    }
+}
+
+__device__ __forceinline__ float2 unpack_yz(float bits) {
+    const unsigned u = __float_as_uint(bits);
+    return __half22float2(*reinterpret_cast<const __half2*>(&u));
+}
+
+// first j in [lo, hi) with rec[j].x >= v / > v (x-sorted rows)
+__device__ __forceinline__ int lower_rx(const float2* __restrict__ r, int lo, int hi, float v) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&r[mid].x) < v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ int upper_rx(const float2* __restrict__ r, int lo, int hi, float v) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&r[mid].x) <= v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+constexpr int kMixThreads = 128;
+
+__global__ void __launch_bounds__(kMixThreads) k_pair_mixed(GridDev g, MixParams mp, const float2* __restrict__ rec,
+                                                            const int* __restrict__ cs, const int* __restrict__ off,
+                                                            int n, float* __restrict__ energy,
+                                                            float* __restrict__ force, Partial* part,
+                                                            unsigned* counter, lj_totals* totals, unsigned* status) {
+    __shared__ int2 s_win[kMaxWin][kMixThreads];
+    __shared__ unsigned char s_row[kMaxWin][kMixThreads];
+    const int tid = threadIdx.x;
+    const int k = blockIdx.x * kMixThreads + tid;
+    float se = 0.f, ce = 0.f, sx = 0.f, cx_ = 0.f, sy = 0.f, cy_ = 0.f, sz = 0.f, cz_ = 0.f, wa = 0.f;
+    unsigned np = 0;
+    if (k < n) {
+        const float2 ri = __ldg(&rec[k]);
+        const float xi = ri.x;
+        const float2 ui = unpack_yz(ri.y);
+        int c = __ldg(&cs[k]);
+        if (c < 0 || c >= g.gx * g.gy * g.gz) {
+            atomicOr(status, kFlagRange);
+            c = 0;
+        }
+        int cx, cy, cz;
+        decode_cell(g, c, cx, cy, cz);
+        const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
+        const float slack = mp.slack + 8.0f * FLT_EPSILON * fabsf(xi);
+        const float slack_u = 1e-5f;
+        int nw = 0;
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+            const int dz = r / 3 - 1, dy = r % 3 - 1;
+            const int z = cz + dz, y = cy + dy;
+            if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) continue;
+            // lower bound of the (y, z) distance to the row, cell units: rows below/above start at the cell faces
+            float dzm = dz < 0 ? ui.y : (dz > 0 ? 1.0f - ui.y : 0.f);
+            float dym = dy < 0 ? ui.x : (dy > 0 ? 1.0f - ui.x : 0.f);
+            dzm = fmaxf(dzm - slack_u, 0.f);
+            dym = fmaxf(dym - slack_u, 0.f);
+            const float d2 = fmaf(dym, dym, dzm * dzm);
+            if (d2 >= mp.rc2uw) continue;
+            const int rb = (z * g.gy + y) * g.gx;
+            int s = min(max(__ldg(&off[rb + xl]), 0), n);
+            int e = min(max(__ldg(&off[rb + xh + 1]), s), n);
+            const float h = sqrtf(mp.rc2uw - d2) * mp.w + slack;
+            s = lower_rx(rec, s, e, xi - h);
+            e = upper_rx(rec, s, e, xi + h);
+            if (r == 4) {
+                s_win[nw][tid] = make_int2(s, k);
+                s_row[nw++][tid] = (unsigned char)r;
+                s_win[nw][tid] = make_int2(k + 1, e);
+                s_row[nw++][tid] = (unsigned char)r;
+            } else {
+                s_win[nw][tid] = make_int2(s, e);
+                s_row[nw++][tid] = (unsigned char)r;
+            }
+        }
+        const float rc2u = mp.rc2u, sig2u = mp.sig2u, invw = mp.invw;
+        // flat walk over the windows (the own row always gives two, so nw >= 2)
+        int w = 0;
+        int2 cur = s_win[0][tid];
+        int r = s_row[0][tid];
+        float ty = ui.x - (float)(r % 3 - 1), tz = ui.y - (float)(r / 3 - 1);
+        float pe = 0.f, px = 0.f, py = 0.f, pz = 0.f;
+        while (true) {
+            if (cur.x >= cur.y) {
+                // window done: add its partial sums with compensation
+                two_sum_add(se, ce, pe);
+                two_sum_add(sx, cx_, px);
+                two_sum_add(sy, cy_, py);
+                two_sum_add(sz, cz_, pz);
+                pe = px = py = pz = 0.f;
+                do {
+                    if (++w >= nw) goto walked;
+                    cur = s_win[w][tid];
+                } while (cur.x >= cur.y);
+                r = s_row[w][tid];
+                ty = ui.x - (float)(r % 3 - 1);
+                tz = ui.y - (float)(r / 3 - 1);
+            }
+            {
+                const float2 q = __ldg(&rec[cur.x]);
+                ++cur.x;
+                const float2 uj = unpack_yz(q.y);
+                const float dx = __fmul_rn(__fsub_rn(q.x, xi), invw);
+                const float dy = __fsub_rn(uj.x, ty);
+                const float dz = __fsub_rn(uj.y, tz);
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                if (r2 < rc2u) {
+                    const float ir2 = rcp_approx(r2);
+                    const float s2 = sig2u * ir2;
+                    const float s6 = s2 * s2 * s2;
+                    const float s12 = s6 * s6;
+                    pe += s12 - s6;
+                    const float t = fmaf(2.0f, s12, -s6);
+                    wa += t;
+                    const float fs = t * s2;
+                    px = fmaf(fs, dx, px);
+                    py = fmaf(fs, dy, py);
+                    pz = fmaf(fs, dz, pz);
+                    ++np;
+                }
+            }
+        }
+    walked:
+        if (energy) energy[k] = mp.e4 * (se + ce);
+        if (force) {
+            force[3 * (size_t)k + 0] = mp.fscale * (sx + cx_);
+            force[3 * (size_t)k + 1] = mp.fscale * (sy + cy_);
+            force[3 * (size_t)k + 2] = mp.fscale * (sz + cz_);
+        }
+    }
+    reduce_totals<kMixThreads>(0.5 * (double)mp.e4 * ((double)se + (double)ce), 0.5 * (double)mp.e24 * (double)wa,
+                               (unsigned long long)np, part, counter, totals);
+}
+
+}  // namespace ljc
+
+using namespace ljc;
+
+extern "C" lj_status lj_pack_mixed(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi,
+                                   const int* sorted_cell, float* rec) {
+    if (!ctx || !g || n < 0 || (n > 0 && (!sorted_xyzi || !sorted_cell || !rec))) return LJ_EINVAL;
+    if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
+    if ((reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) || (reinterpret_cast<uintptr_t>(rec) & 7)) return LJ_EINVAL;
+    if (n == 0) return LJ_OK;
+    int blocks = (n + 255) / 256;
+    if (blocks > ctx->sm_count * 8) blocks = ctx->sm_count * 8;
+    k_pack_mixed<<<blocks, 256, 0, ctx->stream>>>(to_dev(*g), reinterpret_cast<const float4*>(sorted_xyzi),
+                                                  sorted_cell, n, reinterpret_cast<float2*>(rec));
+    return last_launch_status();
+}
+
+extern "C" lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* rec,
+                                      const int* sorted_cell, const int* offsets, float* energy, float* force,
+                                      lj_totals* totals) {
+    if (!ctx || !g || !p || n < 0 || (n > 0 && (!rec || !sorted_cell || !offsets))) return LJ_EINVAL;
+    if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
+    if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;
+    if (reinterpret_cast<uintptr_t>(rec) & 7) return LJ_EINVAL;
+    if (n == 0) {
+        if (totals && cudaMemsetAsync(totals, 0, sizeof(lj_totals), ctx->stream) != cudaSuccess) return LJ_ECUDA;
+        return LJ_OK;
+    }
+    MixParams mp;
+    mp.w = g->width;
+    mp.invw = 1.0f / g->width;
+    const float rc2 = p->cutoff * p->cutoff;
+    mp.rc2u = rc2 * mp.invw * mp.invw;
+    mp.rc2uw = mp.rc2u * (1.0f + 1e-5f);
+    const float sig2 = p->sigma * p->sigma;
+    mp.sig2u = sig2 * mp.invw * mp.invw;
+    mp.e4 = 4.0f * p->epsilon;
+    mp.e24 = 24.0f * p->epsilon;
+    mp.fscale = -mp.e24 * g->width / sig2;
+    mp.slack = grid_slack(*g);
+    const int blocks = (n + kMixThreads - 1) / kMixThreads;
+    const size_t need = 256 + (size_t)blocks * sizeof(Partial);
+    if (need > ctx->red_bytes) {
+        lj_status s = grow(&ctx->red, &ctx->red_bytes, need);
+        if (s != LJ_OK) return s;
+        if (cudaMemsetAsync(ctx->red, 0, 256, ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    }
+    unsigned* counter = static_cast<unsigned*>(ctx->red);
+    Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
+    k_pair_mixed<<<blocks, kMixThreads, 0, ctx->stream>>>(to_dev(*g), mp, reinterpret_cast<const float2*>(rec),
+                                                          sorted_cell, offsets, n, energy, force, part, counter,
+                                                          totals, ctx->d_status);
+    return last_launch_status();
+}

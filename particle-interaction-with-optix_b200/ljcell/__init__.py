@@ -121,6 +121,8 @@ def _load() -> C.CDLL:
         "lj_batch_run_graph": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
         "lj_batch_run_separate": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp]),
         "lj_batch_autotune": (i32, [vp, vp, vp, vp, vp, C.POINTER(BatchConfig), C.POINTER(C.c_float)]),
+        "lj_pack_mixed": (i32, [vp, C.POINTER(Grid), i32, vp, vp, vp]),
+        "lj_compute_mixed": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp]),
         "lj_simulate_host": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
                                    C.POINTER(Totals)]),
     }
@@ -137,7 +139,8 @@ ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj
                "lj_count_cells", "lj_exclusive_scan", "lj_exclusive_scan_noalloc", "lj_cell_descriptors", "lj_bin", "lj_count_candidates",
                "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_autotune_compute", "lj_batch_create",
                "lj_batch_destroy", "lj_batch_get_config", "lj_batch_grid", "lj_batch_run", "lj_batch_run_graph",
-               "lj_batch_run_separate", "lj_batch_autotune", "lj_simulate_host")
+               "lj_batch_run_separate", "lj_batch_autotune", "lj_pack_mixed", "lj_compute_mixed",
+               "lj_simulate_host")
 
 
 def lib() -> C.CDLL:
@@ -367,6 +370,20 @@ class Context:
         _check(_lib.lj_compute(self._h, C.byref(g), C.byref(p), b.n, _ptr(b.xyzi), _ptr(b.cell), _ptr(b.offsets),
                                b.order, _ptr(energy) if want_energy else None,
                                _ptr(force) if want_force else None, _ptr(totals)), "lj_compute")
+        return energy, force, totals
+
+    def pack_mixed(self, g: Grid, b: Binned, rec=None):
+        """Mixed-precision records (n, 2) float32: x and the binary16 pair (uy, uz) bit-packed."""
+        t = self.torch
+        rec = rec if rec is not None else t.empty((max(b.n, 1), 2), dtype=t.float32, device=self.device)
+        _check(_lib.lj_pack_mixed(self._h, C.byref(g), b.n, _ptr(b.xyzi), _ptr(b.cell), _ptr(rec)), "lj_pack_mixed")
+        return rec
+
+    def compute_mixed(self, g: Grid, p: Params, b: Binned, rec, energy=None, force=None, totals=None):
+        if energy is None and force is None and totals is None:
+            energy, force, totals = self.alloc_outputs(b.n)
+        _check(_lib.lj_compute_mixed(self._h, C.byref(g), C.byref(p), b.n, _ptr(rec), _ptr(b.cell), _ptr(b.offsets),
+                                     _ptr(energy), _ptr(force), _ptr(totals)), "lj_compute_mixed")
         return energy, force, totals
 
     def simulate_host(self, g: Grid, p: Params, hx: np.ndarray, hy: np.ndarray, hz: np.ndarray,
