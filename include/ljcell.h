@@ -314,7 +314,9 @@ LJ_API lj_status lj_batch_autotune(lj_ctx* ctx, lj_batch* b, const float* x, con
 /* Records from binned particles (LJ_ORDER_X).  rec: 2n floats, 8-byte aligned. */
 LJ_API lj_status lj_pack_mixed(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi,
                                const int* sorted_cell, float* rec);
-/* Energy, force (sorted order) and totals from the records; as lj_compute. */
+/* Energy, force (sorted order) and totals from the records; as lj_compute.
+ * The tuning's pair_kernel 2 selects the register-window variant; any other
+ * value the shared-memory-window one (the faster of the two on B200). */
 LJ_API lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* rec,
                                   const int* sorted_cell, const int* offsets, float* energy, float* force,
                                   lj_totals* totals);

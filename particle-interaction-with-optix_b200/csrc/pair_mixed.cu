@@ -203,6 +203,119 @@ __global__ void __launch_bounds__(kMixThreads) k_pair_mixed(GridDev g, MixParams
                                (unsigned long long)np, part, counter, totals);
 }
 
+// The same with the windows in registers (slot r = stencil row r, slot 9 =
+// the own row after the target), walked by shifting: no shared memory, so the
+// whole L1 caches neighbour records.  Faster on dense grids, as for the plain
+// form (pair_direct.cu).
+__global__ void __launch_bounds__(kMixThreads) k_pair_mixed_reg(GridDev g, MixParams mp,
+                                                                const float2* __restrict__ rec,
+                                                                const int* __restrict__ cs,
+                                                                const int* __restrict__ off, int n,
+                                                                float* __restrict__ energy, float* __restrict__ force,
+                                                                Partial* part, unsigned* counter, lj_totals* totals,
+                                                                unsigned* status) {
+    const int k = blockIdx.x * kMixThreads + threadIdx.x;
+    float se = 0.f, ce = 0.f, sx = 0.f, cx_ = 0.f, sy = 0.f, cy_ = 0.f, sz = 0.f, cz_ = 0.f, wa = 0.f;
+    unsigned np = 0;
+    if (k < n) {
+        const float2 ri = __ldg(&rec[k]);
+        const float xi = ri.x;
+        const float2 ui = unpack_yz(ri.y);
+        int c = __ldg(&cs[k]);
+        if (c < 0 || c >= g.gx * g.gy * g.gz) {
+            atomicOr(status, kFlagRange);
+            c = 0;
+        }
+        int cx, cy, cz;
+        decode_cell(g, c, cx, cy, cz);
+        const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
+        const float slack = mp.slack + 8.0f * FLT_EPSILON * fabsf(xi);
+        int2 slot[10];
+#pragma unroll
+        for (int i = 0; i < 10; ++i) slot[i] = make_int2(0, 0);
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+            const int dz = r / 3 - 1, dy = r % 3 - 1;
+            const int z = cz + dz, y = cy + dy;
+            if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) continue;
+            float dzm = dz < 0 ? ui.y : (dz > 0 ? 1.0f - ui.y : 0.f);
+            float dym = dy < 0 ? ui.x : (dy > 0 ? 1.0f - ui.x : 0.f);
+            dzm = fmaxf(dzm - 1e-5f, 0.f);
+            dym = fmaxf(dym - 1e-5f, 0.f);
+            const float d2 = fmaf(dym, dym, dzm * dzm);
+            if (d2 >= mp.rc2uw) continue;
+            const int rb = (z * g.gy + y) * g.gx;
+            const int s = min(max(__ldg(&off[rb + xl]), 0), n);
+            const int e = min(max(__ldg(&off[rb + xh + 1]), s), n);
+            const float h = sqrtf(mp.rc2uw - d2) * mp.w + slack;
+            const int lo = lower_rx(rec, s, e, xi - h);
+            const int hi = upper_rx(rec, lo, e, xi + h);
+            if (r == 4) {
+                slot[4] = make_int2(lo, k);
+                slot[9] = make_int2(k + 1, hi);
+            } else {
+                slot[r] = make_int2(lo, hi);
+            }
+        }
+        const float rc2u = mp.rc2u, sig2u = mp.sig2u, invw = mp.invw;
+        int idx = 0;  // slot being walked; its row is idx (idx < 9) or 4 (idx = 9)
+        int2 cur = slot[0];
+        float ty = ui.x + 1.0f, tz = ui.y + 1.0f;  // row 0: dy = dz = -1
+        float pe = 0.f, px = 0.f, py = 0.f, pz = 0.f;
+        while (true) {
+            if (cur.x >= cur.y) {
+                two_sum_add(se, ce, pe);
+                two_sum_add(sx, cx_, px);
+                two_sum_add(sy, cy_, py);
+                two_sum_add(sz, cz_, pz);
+                pe = px = py = pz = 0.f;
+                do {
+                    if (++idx == 10) goto walked;
+                    cur = slot[1];
+#pragma unroll
+                    for (int i = 1; i < 9; ++i) slot[i] = slot[i + 1];
+                    slot[9] = make_int2(0, 0);
+                } while (cur.x >= cur.y);
+                const int row = idx < 9 ? idx : 4;
+                ty = ui.x - (float)(row % 3 - 1);
+                tz = ui.y - (float)(row / 3 - 1);
+            }
+            {
+                const float2 q = __ldg(&rec[cur.x]);
+                ++cur.x;
+                const float2 uj = unpack_yz(q.y);
+                const float dx = __fmul_rn(__fsub_rn(q.x, xi), invw);
+                const float dy = __fsub_rn(uj.x, ty);
+                const float dz = __fsub_rn(uj.y, tz);
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                if (r2 < rc2u) {
+                    const float ir2 = rcp_approx(r2);
+                    const float s2 = sig2u * ir2;
+                    const float s6 = s2 * s2 * s2;
+                    const float s12 = s6 * s6;
+                    pe += s12 - s6;
+                    const float t = fmaf(2.0f, s12, -s6);
+                    wa += t;
+                    const float fs = t * s2;
+                    px = fmaf(fs, dx, px);
+                    py = fmaf(fs, dy, py);
+                    pz = fmaf(fs, dz, pz);
+                    ++np;
+                }
+            }
+        }
+    walked:
+        if (energy) energy[k] = mp.e4 * (se + ce);
+        if (force) {
+            force[3 * (size_t)k + 0] = mp.fscale * (sx + cx_);
+            force[3 * (size_t)k + 1] = mp.fscale * (sy + cy_);
+            force[3 * (size_t)k + 2] = mp.fscale * (sz + cz_);
+        }
+    }
+    reduce_totals<kMixThreads>(0.5 * (double)mp.e4 * ((double)se + (double)ce), 0.5 * (double)mp.e24 * (double)wa,
+                               (unsigned long long)np, part, counter, totals);
+}
+
 }  // namespace ljc
 
 using namespace ljc;
@@ -252,8 +365,15 @@ extern "C" lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_pa
     }
     unsigned* counter = static_cast<unsigned*>(ctx->red);
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
-    k_pair_mixed<<<blocks, kMixThreads, 0, ctx->stream>>>(to_dev(*g), mp, reinterpret_cast<const float2*>(rec),
-                                                          sorted_cell, offsets, n, energy, force, part, counter,
-                                                          totals, ctx->d_status);
+    // windows in shared memory unless pair_kernel 2 asks for registers (measured faster for the mixed
+    // records on sparse and dense grids alike)
+    if (ctx->tuning.pair_kernel == 2)
+        k_pair_mixed_reg<<<blocks, kMixThreads, 0, ctx->stream>>>(to_dev(*g), mp, reinterpret_cast<const float2*>(rec),
+                                                                  sorted_cell, offsets, n, energy, force, part,
+                                                                  counter, totals, ctx->d_status);
+    else
+        k_pair_mixed<<<blocks, kMixThreads, 0, ctx->stream>>>(to_dev(*g), mp, reinterpret_cast<const float2*>(rec),
+                                                              sorted_cell, offsets, n, energy, force, part, counter,
+                                                              totals, ctx->d_status);
     return last_launch_status();
 }

@@ -18,15 +18,18 @@ FORCE_NORMWISE_TOL = 1e-5
 TOTAL_ENERGY_TOL = 1e-6
 
 
+@pytest.mark.parametrize("kernel", [1, 2])   # windows in shared memory / in registers
 @pytest.mark.parametrize("name", ["uniform_c1", "uniform_dense", "shell", "tiny33"])
-def test_mixed_against_oracle(torch_cuda, ctx, name):
+def test_mixed_against_oracle(torch_cuda, ctx, name, kernel):
     import ljcell
 
     (x, y, z), g, og, b, ob, rc = bin_both(torch_cuda, ctx, name, 1)
     p = ljcell.params(rc)
+    ctx.set_tuning(kernel)
     rec = ctx.pack_mixed(g, b)
     e, f, tot = ctx.compute_mixed(g, p, b, rec)
     ctx.sync()
+    ctx.set_tuning(0)
     n = len(x)
     r = np_(rec)[:n]
     uy, uz = O.pack_mixed(og, ob)
