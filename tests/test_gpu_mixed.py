@@ -61,3 +61,45 @@ def test_mixed_deterministic(torch_cuda, ctx):
         outs.append((np_(e), np_(f), np_(tot)))
     for a, c in zip(*outs):
         assert np.array_equal(a.view(np.uint8), c.view(np.uint8))
+
+
+def test_mixed_dense_sample(torch_cuda, ctx):
+    """The dense configuration (10M uniform, rc = 0.02, about 335 neighbours):
+    errors of the mixed form on 50,000 targets against FP64 on the stored
+    positions, and the effect of the binary16 offsets themselves (stored vs
+    unrounded positions), printed for the record."""
+    import ljcell
+
+    torch = torch_cuda
+    n, rc = 10_000_000, 0.02
+    g = ljcell.grid_from_box((0, 0, 0), (1, 1, 1), rc)
+    p = ljcell.params(rc)
+    soa, _ = ctx.generate_uniform(1234, n)
+    b = ctx.bin(g, soa["x"], soa["y"], soa["z"], order=1)
+    rec = ctx.pack_mixed(g, b)
+    e, f, tot = ctx.compute_mixed(g, p, b, rec)
+    ctx.sync()
+    xyzi = np_(b.xyzi)[:n]
+    ob = O.Binned(None, np_(b.offsets), xyzi[:, 3].view(np.int32).copy(), np_(b.cell)[:n].copy(),
+                  np.ascontiguousarray(xyzi[:, 0]), np.ascontiguousarray(xyzi[:, 1]), np.ascontiguousarray(xyzi[:, 2]))
+    og = O.grid_from_box((0, 0, 0), (1, 1, 1), rc)
+    uy, uz = O.pack_mixed(og, ob)
+    k0, k1 = n // 2, n // 2 + 50_000
+    stored = O.mixed_forces(og, ob, uy, uz, rc, 1.0, p.sigma, k0, k1)
+    fe = stored.force_errors(np_(f)[k0:k1])
+    ee = stored.energy_errors(np_(e)[k0:k1])
+    cy = (ob.cell_sorted // og.dim[0]) % og.dim[1]
+    cz = ob.cell_sorted // (og.dim[0] * og.dim[1])
+    w = np.float32(rc)
+    uy32 = ((ob.sy - cy.astype(np.float32) * w) / w).astype(np.float32)
+    uz32 = ((ob.sz - cz.astype(np.float32) * w) / w).astype(np.float32)
+    orig = O.mixed_forces(og, ob, uy32, uz32, rc, 1.0, p.sigma, k0, k1)
+    ok = orig.representable() & stored.representable()
+    q = float(np.linalg.norm(stored.f64[ok] - orig.f64[ok]) / np.linalg.norm(orig.f64[ok]))
+    print(f"mixed dense sample: force normwise {fe['normwise']:.3e} max scaled {fe['max_scaled']:.3e} "
+          f"p99 rel {fe['p99_rel']:.3e}; energy max scaled {ee['max_scaled']:.3e}; "
+          f"binary16 input effect on forces {q:.3e}")
+    assert fe["normwise"] <= FORCE_NORMWISE_TOL and fe["max_scaled"] <= FORCE_SCALED_TOL, fe
+    assert ee["max_scaled"] <= FORCE_SCALED_TOL, ee
+    del soa, b, rec, e, f, tot
+    torch.cuda.empty_cache()
