@@ -183,32 +183,40 @@ __device__ __forceinline__ void pair_target(const GridDev& g, const PairParams& 
     int w = 0;
     int2 cur = s_win[0][tid];
     const float rc2 = pp.rc2, sig2 = pp.sig2;
+    // Two candidates per iteration (the second masked off when the window has one left): half the loop
+    // overhead and two loads in flight.  Candidates are added in window order, as one at a time would.
+    auto body = [&](const float4& q, bool valid) {
+        const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        if (valid && r2 < rc2) {
+            const float ir2 = rcp_approx(r2);
+            const float s2 = sig2 * ir2;
+            const float s6 = s2 * s2 * s2;
+            const float s12 = s6 * s6;
+            ea += s12 - s6;
+            const float t = fmaf(2.0f, s12, -s6);
+            wa += t;
+            // force in units of 24 eps / sigma^2: t * s2 stays finite where t * ir2 would overflow
+            const float fs = t * s2;
+            fx = fmaf(fs, dx, fx);
+            fy = fmaf(fs, dy, fy);
+            fz = fmaf(fs, dz, fz);
+            ++np;
+        }
+    };
     while (true) {
         while (cur.x >= cur.y) {
             if (++w >= nw) return;
             cur = s_win[w][tid];
         }
-        {
-            const float4 q = __ldg(&p[cur.x]);
-            ++cur.x;
-            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            if (r2 < rc2) {
-                const float ir2 = rcp_approx(r2);
-                const float s2 = sig2 * ir2;
-                const float s6 = s2 * s2 * s2;
-                const float s12 = s6 * s6;
-                ea += s12 - s6;
-                const float t = fmaf(2.0f, s12, -s6);
-                wa += t;
-                // force in units of 24 eps / sigma^2: t * s2 stays finite where t * ir2 would overflow
-                const float fs = t * s2;
-                fx = fmaf(fs, dx, fx);
-                fy = fmaf(fs, dy, fy);
-                fz = fmaf(fs, dz, fz);
-                ++np;
-            }
-        }
+        const int j0 = cur.x;
+        const bool two = j0 + 1 < cur.y;
+        const int j1 = two ? j0 + 1 : j0;
+        cur.x = j1 + 1;
+        const float4 q0 = __ldg(&p[j0]);
+        const float4 q1 = __ldg(&p[j1]);
+        body(q0, true);
+        body(q1, two);
     }
 }
 
