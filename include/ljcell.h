@@ -321,6 +321,12 @@ LJ_API lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params
                                   const int* sorted_cell, const int* offsets, float* energy, float* force,
                                   lj_totals* totals);
 
+/* ------------------------------------------------------------- test hook
+ * Failure-path check (no counterpart in the reference): runs the scan with
+ * its first tile withheld, so every bounded look-back wait gives up; the next
+ * lj_sync returns LJ_ETIMEOUT and the context stays usable.  ncells > 4096. */
+LJ_API lj_status lj_test_scan_withheld_tile(lj_ctx* ctx, const int* counts, long long ncells, int* offsets);
+
 /* ------------------------------------------------------------- end to end
  * One call with HOST buffers, the shape of executeSimulation's step
  * (cudaLJ.cu:613-653) without the generation: copies positions to the device,

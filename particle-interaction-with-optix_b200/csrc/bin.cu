@@ -65,7 +65,7 @@ constexpr int kScanTile = 4096;
 constexpr unsigned long long kStAgg = 1ULL << 62;
 constexpr unsigned long long kStPre = 2ULL << 62;
 constexpr unsigned long long kStVal = (1ULL << 62) - 1ULL;
-constexpr unsigned kSpinLimit = 1u << 22;
+constexpr unsigned kSpinLimit = 1u << 20;  // polls: well under a second of waiting
 
 __device__ __forceinline__ unsigned long long ld_state(const unsigned long long* p) {
     return *reinterpret_cast<const volatile unsigned long long*>(p);
@@ -597,6 +597,30 @@ extern "C" lj_status lj_count_candidates(lj_ctx* ctx, const lj_grid* g, const in
     if (s != LJ_OK) return s;
     if (cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), ctx->stream) != cudaSuccess) return LJ_ECUDA;
     k_candidates<<<grid_for(ctx, nc, 256), 256, 0, ctx->stream>>>(to_dev(*g), offsets, nc, d_count);
+    return last_launch_status();
+}
+
+// ---------------------------------------------------------------- failure-path test hook
+namespace ljc {
+__global__ void k_set_u32(unsigned* p, unsigned v) { *p = v; }
+}  // namespace ljc
+
+// Runs k_scan with tile 0 withheld: the counter starts at 1, so no CTA ever
+// publishes tile 0 and every look-back wait runs out its bounded limit,
+// records LJ_ETIMEOUT in the context's status word and returns.  Exercises the
+// error path of the bounded waits without faulting or hanging the GPU.
+extern "C" lj_status lj_test_scan_withheld_tile(lj_ctx* ctx, const int* counts, long long ncells, int* offsets) {
+    if (!ctx || !counts || !offsets || ncells <= kScanTile || ncells > (long long)INT_MAX - 1) return LJ_EINVAL;
+    const long long ntiles = (ncells + kScanTile - 1) / kScanTile;
+    const size_t need = 256 + (size_t)ntiles * sizeof(unsigned long long);
+    lj_status s = grow(&ctx->scan_state, &ctx->scan_state_bytes, need);
+    if (s != LJ_OK) return s;
+    if (cudaMemsetAsync(ctx->scan_state, 0, need, ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    unsigned* counter = reinterpret_cast<unsigned*>(ctx->scan_state);
+    unsigned long long* states = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->scan_state) + 256);
+    k_set_u32<<<1, 1, 0, ctx->stream>>>(counter, 1u);
+    k_scan<<<(unsigned)(ntiles - 1), kScanThreads, 0, ctx->stream>>>(counts, offsets, ncells, ntiles, states, counter,
+                                                                      0, ctx->d_status);
     return last_launch_status();
 }
 

@@ -25,7 +25,7 @@
 namespace ljc {
 
 constexpr int kTileThreads = 256;
-constexpr unsigned kMbarSpinLimit = 1u << 22;
+constexpr unsigned kMbarSpinLimit = 1u << 20;  // try_wait polls: about a second at most
 
 extern __shared__ float4 s_stage[];
 
