@@ -109,6 +109,11 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->red);
     cudaFree(c->tiles);
     cudaFree(c->e2e);
+    if (c->e2e_ready) {
+        cudaStreamSynchronize(c->copy_stream);
+        for (int i = 0; i < 8; ++i) cudaEventDestroy(c->e2e_ev[i]);
+        cudaStreamDestroy(c->copy_stream);
+    }
     delete c;
     return LJ_OK;
 }
@@ -169,14 +174,52 @@ extern "C" lj_status lj_grid_compat(float box_width, float cutoff, lj_grid* out)
     return lj_grid_from_box(lo, hi, cutoff, out);
 }
 
+namespace ljc {
+
+// The pair stage of lj_simulate_host runs in this many target chunks, so that each chunk's
+// device-to-host copy of energy / force overlaps the next chunk's compute.
+constexpr int kE2EChunks = 4;
+
+// Totals of the chunks, summed in chunk order (deterministic).
+__global__ void k_sum_totals(const lj_totals* __restrict__ part, int nparts, lj_totals* __restrict__ out) {
+    double e = 0.0, w = 0.0;
+    unsigned long long np = 0;
+    for (int i = 0; i < nparts; ++i) {
+        e += part[i].energy;
+        w += part[i].virial;
+        np += part[i].pairs;
+    }
+    *out = lj_totals{e, w, np, 0ULL};
+}
+
+lj_status e2e_setup(lj_ctx* c) {
+    if (c->e2e_ready) return LJ_OK;
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) return LJ_ECUDA;
+    for (int i = 0; i < 8; ++i)
+        if (cudaEventCreateWithFlags(&c->e2e_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            for (int j = 0; j < i; ++j) cudaEventDestroy(c->e2e_ev[j]);
+            cudaStreamDestroy(c->copy_stream);
+            c->copy_stream = nullptr;
+            return LJ_ECUDA;
+        }
+    c->e2e_ready = true;
+    return LJ_OK;
+}
+
+}  // namespace ljc
+
 extern "C" lj_status lj_simulate_host(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx,
                                       const float* hy, const float* hz, float* h_energy, float* h_force,
                                       int* h_index, lj_totals* h_totals) {
     if (!c || !g || !p || n < 0 || (n > 0 && (!hx || !hy || !hz))) return LJ_EINVAL;
+    if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
+    if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;
     DeviceScope scope(c->device);
     if (!scope.ok) return LJ_ECUDA;
     const long long nc = (long long)g->dim[0] * g->dim[1] * g->dim[2];
     if (nc < 1 || nc > 2147483646LL) return LJ_EINVAL;
+    lj_status s = e2e_setup(c);
+    if (s != LJ_OK) return s;
     const size_t N = (size_t)(n > 0 ? n : 1);
     auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t b_pos = up(3 * N * sizeof(float));
@@ -187,9 +230,9 @@ extern "C" lj_status lj_simulate_host(lj_ctx* c, const lj_grid* g, const lj_para
     const size_t b_e = up(N * sizeof(float));
     const size_t b_f = up(3 * N * sizeof(float));
     const size_t b_idx = up(N * sizeof(int));
-    const size_t b_tot = up(sizeof(lj_totals));
+    const size_t b_tot = up((kE2EChunks + 1) * sizeof(lj_totals));
     const size_t need = b_pos + b_cnt + b_off + b_x4 + b_cell + b_e + b_f + b_idx + b_tot;
-    lj_status s = grow(&c->e2e, &c->e2e_bytes, need);
+    s = grow(&c->e2e, &c->e2e_bytes, need);
     if (s != LJ_OK) return s;
     char* base = static_cast<char*>(c->e2e);
     float* dpos = reinterpret_cast<float*>(base);
@@ -209,7 +252,12 @@ extern "C" lj_status lj_simulate_host(lj_ctx* c, const lj_grid* g, const lj_para
     int* didx = reinterpret_cast<int*>(base);
     base += b_idx;
     lj_totals* dtot = reinterpret_cast<lj_totals*>(base);
-    cudaStream_t st = c->stream;
+    cudaStream_t st = c->stream, cp = c->copy_stream;
+    // every return leaves no copy in flight into the caller's host buffers
+    struct Drain {
+        cudaStream_t s;
+        ~Drain() { cudaStreamSynchronize(s); }
+    } drain{cp};
     const size_t pb = (size_t)n * sizeof(float);
     if (n > 0) {
         if (cudaMemcpyAsync(dpos, hx, pb, cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -221,18 +269,37 @@ extern "C" lj_status lj_simulate_host(lj_ctx* c, const lj_grid* g, const lj_para
     sorted.index = didx;
     s = lj_bin(c, g, n, dpos, dpos + N, dpos + 2 * N, 1, LJ_ORDER_X, dcnt, doff, nullptr, &sorted, dx4, dcell);
     if (s != LJ_OK) return s;
-    s = lj_compute(c, g, p, n, dx4, dcell, doff, LJ_ORDER_X, h_energy ? de : nullptr, h_force ? df : nullptr, dtot);
-    if (s != LJ_OK) return s;
-    if (n > 0) {
-        if (h_energy && cudaMemcpyAsync(h_energy, de, pb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    // The index is final once binning is done: copy it back while the pair stage runs.
+    if (cudaEventRecord(c->e2e_ev[0], st) != cudaSuccess || cudaStreamWaitEvent(cp, c->e2e_ev[0], 0) != cudaSuccess)
+        return LJ_ECUDA;
+    if (n > 0 && h_index &&
+        cudaMemcpyAsync(h_index, didx, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, cp) != cudaSuccess)
+        return LJ_ECUDA;
+    // Pair stage in target chunks; chunk k's outputs go back on the copy stream during chunk k + 1.
+    // The tiled kernel (tuning 4) covers whole ranges only, so it runs as one chunk.
+    const int chunks = (c->tuning.pair_kernel == 4 || n < kE2EChunks * 4096) ? 1 : kE2EChunks;
+    for (int k = 0; k < chunks; ++k) {
+        const int kb = (int)((long long)n * k / chunks), ke = (int)((long long)n * (k + 1) / chunks);
+        s = launch_pair_config(c, g, p, n, dx4, dcell, doff, LJ_ORDER_X, h_energy ? de : nullptr,
+                               h_force ? df : nullptr, dtot + k, kb, ke);
+        if (s != LJ_OK) return s;
+        if (ke == kb) continue;
+        if (cudaEventRecord(c->e2e_ev[1 + k], st) != cudaSuccess ||
+            cudaStreamWaitEvent(cp, c->e2e_ev[1 + k], 0) != cudaSuccess)
             return LJ_ECUDA;
-        if (h_force && cudaMemcpyAsync(h_force, df, 3 * pb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        const size_t cb = (size_t)(ke - kb) * sizeof(float);
+        if (h_energy && cudaMemcpyAsync(h_energy + kb, de + kb, cb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
             return LJ_ECUDA;
-        if (h_index && cudaMemcpyAsync(h_index, didx, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st) !=
-                           cudaSuccess)
+        if (h_force &&
+            cudaMemcpyAsync(h_force + 3 * (size_t)kb, df + 3 * (size_t)kb, 3 * cb, cudaMemcpyDeviceToHost, cp) !=
+                cudaSuccess)
             return LJ_ECUDA;
     }
-    if (h_totals && cudaMemcpyAsync(h_totals, dtot, sizeof(lj_totals), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    k_sum_totals<<<1, 1, 0, st>>>(dtot, chunks, dtot + kE2EChunks);
+    if ((s = last_launch_status()) != LJ_OK) return s;
+    if (h_totals &&
+        cudaMemcpyAsync(h_totals, dtot + kE2EChunks, sizeof(lj_totals), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return LJ_ECUDA;
+    if (cudaStreamSynchronize(cp) != cudaSuccess) return LJ_ECUDA;
     return lj_sync(c);
 }

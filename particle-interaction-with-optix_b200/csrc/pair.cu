@@ -30,15 +30,15 @@ constexpr double kDenseCell = 32.0;  // particles per cell above which the defau
 template <bool XWIN>
 __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairParams pp, const float4* __restrict__ p,
                                                               const int* __restrict__ cs,
-                                                              const int* __restrict__ off, int n,
+                                                              const int* __restrict__ off, int n, int kb, int ke,
                                                               float* __restrict__ energy, float* __restrict__ force,
                                                               Partial* part, unsigned* counter, lj_totals* totals,
                                                               unsigned* status) {
     __shared__ int2 s_win[kMaxWin][kPairThreads];
-    const int k = blockIdx.x * kPairThreads + threadIdx.x;
+    const int k = kb + blockIdx.x * kPairThreads + threadIdx.x;   // targets [kb, ke) of the n sorted particles
     float ea = 0.f, fx = 0.f, fy = 0.f, fz = 0.f, wa = 0.f;
     unsigned np = 0;
-    if (k < n) {
+    if (k < ke) {
         int c = cs[k];
         if (c < 0 || c >= g.gx * g.gy * g.gz) {
             atomicOr(status, kFlagRange);
@@ -102,8 +102,10 @@ float grid_slack(const lj_grid& g) {
 
 lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm, int n, const float* xyzi,
                              const int* cs, const int* off, lj_order order, float* energy, float* force,
-                             lj_totals* totals) {
-    if (n == 0) {
+                             lj_totals* totals, int kb, int ke) {
+    if (ke < 0) ke = n;
+    if (kb < 0 || kb > ke || ke > n) return LJ_EINVAL;
+    if (kb == ke) {
         if (totals && cudaMemsetAsync(totals, 0, sizeof(lj_totals), ctx->stream) != cudaSuccess) return LJ_ECUDA;
         return LJ_OK;
     }
@@ -124,13 +126,15 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
             kernel = per_cell >= kDenseCell ? 2 : 1;
         }
         switch (kernel) {
-            case 4: return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
-            case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals);
-            case 2: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals);
+            case 4:  // cell-block tiles cover whole target ranges only; a sub-range runs kernel 1
+                if (kb == 0 && ke == n) return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
+                break;
+            case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);
+            case 2: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals, kb, ke);
             default: break;  // 1: windows in shared memory (below)
         }
     }
-    const int blocks = (n + kPairThreads - 1) / kPairThreads;
+    const int blocks = (ke - kb + kPairThreads - 1) / kPairThreads;
     const size_t need = 256 + (size_t)blocks * sizeof(Partial);
     if (need > ctx->red_bytes) {
         lj_status s = grow(&ctx->red, &ctx->red_bytes, need);
@@ -141,11 +145,12 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
     const float4* p4 = reinterpret_cast<const float4*>(xyzi);
     if (order == LJ_ORDER_X)
-        k_pair_config<true><<<blocks, kPairThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, energy, force,
-                                                                      part, counter, totals, ctx->d_status);
+        k_pair_config<true><<<blocks, kPairThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, kb, ke, energy,
+                                                                      force, part, counter, totals, ctx->d_status);
     else
-        k_pair_config<false><<<blocks, kPairThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, energy,
-                                                                       force, part, counter, totals, ctx->d_status);
+        k_pair_config<false><<<blocks, kPairThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, kb, ke,
+                                                                       energy, force, part, counter, totals,
+                                                                       ctx->d_status);
     return last_launch_status();
 }
 
@@ -173,7 +178,7 @@ extern "C" lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* 
     if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;
     if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
     if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
-    return launch_pair_config(ctx, g, p, n, sorted_xyzi, sorted_cell, offsets, order, energy, force, totals);
+    return launch_pair_config(ctx, g, p, n, sorted_xyzi, sorted_cell, offsets, order, energy, force, totals, 0, n);
 }
 
 extern "C" lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,

@@ -223,7 +223,7 @@ __device__ __forceinline__ void pair_target(const GridDev& g, const PairParams& 
 float grid_slack(const lj_grid& g);
 lj_status launch_pair_direct(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                              const int* cs, const int* off, bool compact, float* energy, float* force,
-                             lj_totals* totals);
+                             lj_totals* totals, int kb, int ke);
 lj_status launch_pair_tiled(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                             const int* off, float* energy, float* force, lj_totals* totals);
 

@@ -57,14 +57,14 @@ __device__ __forceinline__ void drain_queue(float4 (*s_q)[kDirThreads], int qn, 
 template <bool COMPACT>
 __global__ void __launch_bounds__(kDirThreads) k_pair_direct(GridDev g, PairParams pp, const float4* __restrict__ p,
                                                              const int* __restrict__ cs,
-                                                             const int* __restrict__ off, int n,
+                                                             const int* __restrict__ off, int n, int kb, int ke,
                                                              float* __restrict__ energy, float* __restrict__ force,
                                                              Partial* part, unsigned* counter, lj_totals* totals,
                                                              unsigned* status) {
     __shared__ float4 s_q[COMPACT ? kQueue : 1][kDirThreads];
     const int tid = threadIdx.x;
-    const int k = blockIdx.x * kDirThreads + tid;
-    const bool active = k < n;
+    const int k = kb + blockIdx.x * kDirThreads + tid;   // targets [kb, ke) of the n sorted particles
+    const bool active = k < ke;
     DirAcc a{0.f, 0.f, 0.f, 0.f, 0.f, 0u};
     int2 slot[10];
 #pragma unroll
@@ -178,8 +178,8 @@ __global__ void __launch_bounds__(kDirThreads) k_pair_direct(GridDev g, PairPara
 
 lj_status launch_pair_direct(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                              const int* cs, const int* off, bool compact, float* energy, float* force,
-                             lj_totals* totals) {
-    const int blocks = (n + kDirThreads - 1) / kDirThreads;
+                             lj_totals* totals, int kb, int ke) {
+    const int blocks = (ke - kb + kDirThreads - 1) / kDirThreads;
     const size_t need = 256 + (size_t)blocks * sizeof(Partial);
     if (need > ctx->red_bytes) {
         lj_status s = grow(&ctx->red, &ctx->red_bytes, need);
@@ -190,11 +190,11 @@ lj_status launch_pair_direct(lj_ctx* ctx, const lj_grid* g, const PairParams& pp
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
     const float4* p4 = reinterpret_cast<const float4*>(xyzi);
     if (compact)
-        k_pair_direct<true><<<blocks, kDirThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, energy, force,
-                                                                     part, counter, totals, ctx->d_status);
+        k_pair_direct<true><<<blocks, kDirThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, kb, ke, energy,
+                                                                     force, part, counter, totals, ctx->d_status);
     else
-        k_pair_direct<false><<<blocks, kDirThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, energy, force,
-                                                                      part, counter, totals, ctx->d_status);
+        k_pair_direct<false><<<blocks, kDirThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, kb, ke, energy,
+                                                                      force, part, counter, totals, ctx->d_status);
     return last_launch_status();
 }
 

@@ -313,25 +313,36 @@ def test_deterministic(torch_cuda, ctx, kernel):
         assert np.array_equal(a.view(np.uint8), c.view(np.uint8))
 
 
-def test_simulate_host_matches_device_path(torch_cuda, ctx):
+@pytest.mark.parametrize("name,kernel", [("uniform_c1", 0), ("uniform_c1", 1), ("uniform_c1", 2), ("uniform_c1", 3),
+                                         ("uniform_c1", 4), ("tiny33", 0)])
+def test_simulate_host_matches_device_path(torch_cuda, ctx, name, kernel):
+    """The host entry runs the pair stage in target chunks (one chunk for small
+    n and for the tiled kernel); per-particle outputs equal one full-range
+    device call bit for bit, totals to FP64 rounding of the chunk sum."""
     import ljcell
 
     torch = torch_cuda
-    (x, y, z), (lo, hi), rc = case_positions("uniform_c1")
+    (x, y, z), (lo, hi), rc = case_positions(name)
     n = len(x)
     g = ljcell.grid_from_box(lo, hi, rc)
     p = ljcell.params(rc)
     he = np.empty(n, np.float32)
     hf = np.empty((n, 3), np.float32)
     hi_ = np.empty(n, np.int32)
-    tot = ctx.simulate_host(g, p, x, y, z, he, hf, hi_)
-    b = ctx.bin(g, dev(torch, x), dev(torch, y), dev(torch, z), order=1)
-    e, f, t2 = ctx.compute(g, p, b)
-    ctx.sync()
+    ctx.set_tuning(kernel)
+    try:
+        tot = ctx.simulate_host(g, p, x, y, z, he, hf, hi_)
+        b = ctx.bin(g, dev(torch, x), dev(torch, y), dev(torch, z), order=1)
+        e, f, t2 = ctx.compute(g, p, b)
+        ctx.sync()
+    finally:
+        ctx.set_tuning(0)
     np.testing.assert_array_equal(he, np_(e)[:n])
     np.testing.assert_array_equal(hf, np_(f)[:n])
     np.testing.assert_array_equal(hi_, np_(b.xyzi)[:n, 3].view(np.int32))
-    assert tot.pairs == ljcell.totals_from_tensor(t2)["pairs"]
+    t2 = ljcell.totals_from_tensor(t2)
+    assert tot.pairs == t2["pairs"]
+    assert abs(tot.energy - t2["energy"]) <= 1e-12 * max(abs(t2["energy"]), 1e-300)
 
 
 def test_autotune_compute_picks_a_kernel_and_keeps_results(torch_cuda, ctx):
