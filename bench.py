@@ -42,7 +42,10 @@ sys.path.insert(0, os.path.join(ROOT, "particle-interaction-with-optix_b200"))
 METRIC = "LJ pairs/sec @10M particles, plain vs mixed-precision/batched at ≤1e-5 err"
 FLOP_CANDIDATE = 8
 FLOP_INTERACTING = 18
-KERNEL_NAMES = {1: "k_pair_config", 2: "k_pair_direct<false>", 3: "k_pair_direct<true>"}
+KERNEL_NAMES = {1: "k_pair_config", 2: "k_pair_direct<false>", 3: "k_pair_direct<true>", 5: "k_pair_pass<0>",
+                6: "k_pair_pass<1>", 7: "k_pair_pass<2>"}
+# launches of the pair stage per lj_compute call (kernel 7 first copies x, y, z to SoA arrays)
+PAIR_LAUNCHES = {7: 2}
 
 CONFIGS = {
     "c1": dict(workload="uniform 100k, rc=0.05", n=100_000, dist="uniform", lo=(0, 0, 0), hi=(1, 1, 1), rc=0.05),
@@ -364,7 +367,7 @@ def run_ours(args, cfg):
                                         "SM clock; MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
                          "algorithmic_flops": algo_flops},
             "e2e": e2e,
-            "gpu_launches": 6 * K,
+            "gpu_launches": (5 + PAIR_LAUNCHES.get(pair_kernel, 1)) * K,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         }
         if cpu:

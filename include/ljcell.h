@@ -220,21 +220,28 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  * whose launch shape is fixed at 128 threads per particle, cudaLJ.cu:519-520).
  * Results do not depend on them except in the last bits of floating-point
  * sums.  pair_kernel, for particles binned with LJ_ORDER_X:
- *   0 = default: 2 when the grid averages 32 or more particles per cell, else 1,
+ *   0 = default: 7 when the grid averages 32 or more particles per cell, else 6,
  *   1 = direct: one thread per target, neighbours through L1, its windows
  *       in shared memory,
  *   2 = direct with the windows in registers,
  *   3 = direct with compaction: interacting neighbours queued per lane and
  *       the pair law evaluated only for them,
  *   4 = tiled: cell-block tiles staged in shared memory by TMA bulk copies
- *       (totals summed in tile order: not bitwise reproducible run to run). */
+ *       (totals summed in tile order: not bitwise reproducible run to run),
+ *   5 = row passes: the 9 stencil rows walked in 5 warp-synchronous passes
+ *       (opposite rows paired), coalesced neighbour loads, no divergence,
+ *   6 = row passes with two candidates per step in paired FP32 instructions,
+ *   7 = as 6, neighbours read from SoA copies of x, y, z in even-aligned
+ *       pairs (one 8-byte load per coordinate pair; the copy is made per call).
+ * With a non-finite coordinate (reported as LJ_ERANGE) the outputs of the
+ * particles whose windows hold it are unspecified under 5-7. */
 typedef struct {
     int pair_kernel;
     int reserved[7];
 } lj_tuning;
 
 LJ_API lj_status lj_set_tuning(lj_ctx* ctx, const lj_tuning* t);
-/* Autotuner for one system: times the deterministic pair kernels (1-3) on
+/* Autotuner for one system: times the deterministic pair kernels (1-3, 5-7) on
  * these binned (LJ_ORDER_X) particles and keeps the fastest in the context's
  * tuning.  Synchronises. */
 LJ_API lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,

@@ -18,7 +18,7 @@
 #include <new>
 #include <vector>
 
-#include "pair_common.cuh"
+#include "pair_pass.cuh"
 
 namespace ljc {
 
@@ -28,6 +28,8 @@ struct SysDev {
     int cell_base;
     int first;
     int n;
+    int walk;      // pass_target mode: 1 = float4 neighbours, 2 = SoA pairs (the single-system default's choice)
+    int soa_base;  // even start of the system's x / y / z in the SoA copies
 };
 
 // ---------------------------------------------------------------- count
@@ -72,17 +74,20 @@ __global__ void __launch_bounds__(256) k_count_batched(const SysDev* __restrict_
 
 // ---------------------------------------------------------------- pair (persistent, tile queue)
 // Tile = (system, k0, k1): targets [k0, k1) of one system, at most
-// BLOCK * PPT of them.  Per-target raw sums go to te / tw / tnp for the
-// per-system totals.
-template <int BLOCK, int PPT>
+// BLOCK * PPT of them.  Each target runs the single-system default's
+// per-target routine (pass_target, in the system's local indices), so
+// per-particle results equal a per-system lj_compute bit for bit.  One launch
+// per walk mode (MODE), over the tiles of the systems using it.  Per-target
+// raw sums go to te / tw / tnp for the per-system totals.
+template <int BLOCK, int PPT, int MODE>
 __global__ void __launch_bounds__(BLOCK) k_pair_batched(const SysDev* __restrict__ sys, const float4* __restrict__ p,
+                                                        const float* __restrict__ soa, int soa_ld,
                                                         const int* __restrict__ cs, const int* __restrict__ off,
-                                                        int ntotal, const int4* __restrict__ tiles, int ntiles,
+                                                        const int4* __restrict__ tiles, int ntiles,
                                                         unsigned* tile_counter, float* __restrict__ energy,
                                                         float* __restrict__ force, float* __restrict__ te,
                                                         float* __restrict__ tw, unsigned* __restrict__ tnp,
                                                         unsigned* status) {
-    __shared__ int2 s_win[kMaxWin][BLOCK];
     __shared__ int s_t;
     while (true) {
         if (threadIdx.x == 0) s_t = (int)atomicAdd(tile_counter, 1u);
@@ -92,31 +97,64 @@ __global__ void __launch_bounds__(BLOCK) k_pair_batched(const SysDev* __restrict
         const int4 d = __ldg(&tiles[t]);
         const SysDev S = sys[d.x];
         const int ncell = S.g.gx * S.g.gy * S.g.gz;
+        const float4* ps = p + S.first;
+        const float2* x2 = reinterpret_cast<const float2*>(soa + S.soa_base);
+        const float2* y2 = reinterpret_cast<const float2*>(soa + soa_ld + S.soa_base);
+        const float2* z2 = reinterpret_cast<const float2*>(soa + 2 * (size_t)soa_ld + S.soa_base);
 #pragma unroll
         for (int r = 0; r < PPT; ++r) {
             const int k = d.y + r * BLOCK + threadIdx.x;
-            if (k < d.z) {
-                int c = __ldg(&cs[k]) - S.cell_base;
+            const bool active = k < d.z;
+            int c = 0;
+            if (active) {
+                c = __ldg(&cs[k]) - S.cell_base;
                 if (c < 0 || c >= ncell) {
                     atomicOr(status, kFlagRange);
                     c = 0;
                 }
-                float ea = 0.f, fx = 0.f, fy = 0.f, fz = 0.f, wa = 0.f;
-                unsigned np = 0;
-                pair_target<true, BLOCK>(S.g, S.pp, p, off + S.cell_base, ntotal, k, c, s_win, ea, fx, fy, fz, wa,
-                                         np);
+            }
+            PassAcc a;
+            pass_target<MODE>(S.g, S.pp, ps, x2, y2, z2, off + S.cell_base, S.first, S.n, k - S.first, c, active, a);
+            if (active) {
+                const float ea = a.e.x + a.e.y;
                 if (energy) energy[k] = S.pp.e4 * ea;
                 if (force) {
-                    force[3 * (size_t)k + 0] = S.pp.fscale * fx;
-                    force[3 * (size_t)k + 1] = S.pp.fscale * fy;
-                    force[3 * (size_t)k + 2] = S.pp.fscale * fz;
+                    const float nf = -S.pp.fscale;
+                    force[3 * (size_t)k + 0] = nf * (a.fx.x + a.fx.y);
+                    force[3 * (size_t)k + 1] = nf * (a.fy.x + a.fy.y);
+                    force[3 * (size_t)k + 2] = nf * (a.fz.x + a.fz.y);
                 }
                 te[k] = ea;
-                tw[k] = wa;
-                tnp[k] = np;
+                tw[k] = a.w.x + a.w.y;
+                tnp[k] = a.np;
             }
         }
-        __syncthreads();  // s_t and s_win are reused by the next tile
+        __syncthreads();  // s_t is reused by the next tile
+    }
+}
+
+// SoA copies of the sorted positions of the systems that read neighbours as SoA pairs, each system
+// at its even soa_base (the zero pads between systems are set once when the plan is built).
+__global__ void __launch_bounds__(256) k_split_soa_batched(const SysDev* __restrict__ sys,
+                                                           const int* __restrict__ firsts, int nsys,
+                                                           const float4* __restrict__ p, int n, int ld,
+                                                           float* __restrict__ soa) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int lo = 0, hi = nsys - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&firsts[mid]) <= i)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const SysDev& S = sys[lo];
+        if (S.walk != 2) continue;
+        const float4 q = p[i];
+        const int j = S.soa_base + (i - S.first);
+        soa[j] = q.x;
+        soa[ld + j] = q.y;
+        soa[2 * (size_t)ld + j] = q.z;
     }
 }
 
@@ -178,6 +216,7 @@ struct lj_batch {
     int* d_firsts = nullptr;
     int4* d_tiles = nullptr;
     int ntiles = 0;
+    int ntiles1 = 0;  // tiles [0, ntiles1) use walk mode 1, the rest mode 2
     size_t tiles_cap = 0;
     unsigned* d_counter = nullptr;
     int* counts = nullptr;
@@ -188,7 +227,11 @@ struct lj_batch {
     float* te = nullptr;
     float* tw = nullptr;
     unsigned* tnp = nullptr;
-    int persistent_blocks = 0;
+    float* soa = nullptr;  // x, y, z of systems that read SoA pairs, leading dimension soa_ld
+    int soa_ld = 0;
+    int soa_need = 0;
+    bool any_soa = false;
+    int persistent_blocks[2] = {0, 0};  // grid of the persistent pair kernel per walk mode
     // graph replay
     cudaStream_t gstream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -211,6 +254,9 @@ static void free_plan_buffers(lj_batch* b) {
     cudaFree(b->te);
     cudaFree(b->tw);
     cudaFree(b->tnp);
+    cudaFree(b->soa);
+    b->soa = nullptr;
+    b->soa_ld = 0;
     b->d_sys = nullptr;
     b->d_firsts = nullptr;
     b->d_tiles = nullptr;
@@ -232,7 +278,8 @@ static bool valid_config(const lj_batch_config& c) {
 static lj_status build_grids(lj_batch* b) {
     b->grids.resize(b->nsys);
     b->sd.resize(b->nsys);
-    long long base = 0;
+    b->any_soa = false;
+    long long base = 0, soa = 0;
     for (int s = 0; s < b->nsys; ++s) {
         const lj_system& y = b->sys[s];
         const float w = y.params.cutoff * b->cfg.cell_multiple;
@@ -251,15 +298,21 @@ static lj_status build_grids(lj_batch* b) {
         d.cell_base = (int)base;
         d.first = y.first;
         d.n = y.n;
+        d.walk = default_pair_kernel(y.n, g) == 7 ? 2 : 1;
+        d.soa_base = (int)soa;
+        soa += ((long long)y.n + 2 + 1) & ~1LL;
+        if (d.walk == 2) b->any_soa = true;
         base += (long long)g.dim[0] * g.dim[1] * g.dim[2];
-        if (base > 2147483646LL) return LJ_EUNSUPPORTED;
+        if (base > 2147483646LL || soa > 2147483646LL) return LJ_EUNSUPPORTED;
     }
     b->total_cells = base;
+    b->soa_need = (int)((soa + 63) & ~63LL);
     return LJ_OK;
 }
 
-// Tiles of T = threads * per_thread consecutive targets per system, ordered by
-// estimated cost (targets x expected candidates: n / box volume x cutoff^3).
+// Tiles of T = threads * per_thread consecutive targets per system: first those of the systems
+// walked with mode 1, then mode 2, each group ordered by estimated cost (targets x expected
+// candidates: n / box volume x cutoff^3), largest first.
 static std::vector<int4> build_tiles(const lj_batch* b) {
     const int T = b->cfg.threads * b->cfg.per_thread;
     std::vector<std::pair<double, int4>> v;
@@ -274,11 +327,20 @@ static std::vector<int4> build_tiles(const lj_batch* b) {
             v.push_back({per_target * (k1 - k0), make_int4(s, y.first + k0, y.first + k1, 0)});
         }
     }
-    std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& c) { return a.first > c.first; });
+    std::stable_sort(v.begin(), v.end(), [b](const auto& a, const auto& c) {
+        const int wa = b->sd[a.second.x].walk, wc = b->sd[c.second.x].walk;
+        return wa != wc ? wa < wc : a.first > c.first;
+    });
     std::vector<int4> out;
     out.reserve(v.size());
     for (auto& e : v) out.push_back(e.second);
     return out;
+}
+
+static int count_mode1_tiles(const lj_batch* b, const std::vector<int4>& tiles) {
+    int m = 0;
+    while (m < (int)tiles.size() && b->sd[tiles[m].x].walk == 1) ++m;
+    return m;
 }
 
 template <class T>
@@ -291,7 +353,7 @@ static lj_status dev_alloc(T** p, size_t count) {
     return LJ_OK;
 }
 
-static int batched_occupancy(int threads, int ppt);
+static int batched_occupancy(int threads, int ppt, int mode);
 
 // (Re)builds the device side of the plan for b->cfg.  Synchronous.
 static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
@@ -306,6 +368,11 @@ static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
             (st = dev_alloc(&b->d_firsts, (size_t)b->nsys)) != LJ_OK ||
             (st = dev_alloc(&b->d_counter, (size_t)64)) != LJ_OK)
             return st;
+    }
+    if (!b->soa) {
+        if ((st = dev_alloc(&b->soa, 3 * (size_t)b->soa_need)) != LJ_OK) return st;
+        if (cudaMemset(b->soa, 0, 3 * (size_t)b->soa_need * sizeof(float)) != cudaSuccess) return LJ_ECUDA;
+        b->soa_ld = b->soa_need;
     }
     if ((size_t)b->total_cells + 1 > b->cells_cap) {
         cudaFree(b->counts);
@@ -329,7 +396,9 @@ static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
                                       cudaMemcpyHostToDevice) != cudaSuccess))
         return LJ_ECUDA;
     b->ntiles = (int)tiles.size();
-    b->persistent_blocks = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread);
+    b->ntiles1 = count_mode1_tiles(b, tiles);
+    b->persistent_blocks[0] = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread, 1);
+    b->persistent_blocks[1] = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread, 2);
     ++b->version;
     return LJ_OK;
 }
@@ -338,10 +407,11 @@ static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
 
 namespace ljc {
 
-template <int BLOCK, int PPT>
+template <int BLOCK, int PPT, int MODE>
 static int occ_of() {
     int per = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_batched<BLOCK, PPT>, BLOCK, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_batched<BLOCK, PPT, MODE>, BLOCK, 0) !=
+            cudaSuccess ||
         per < 1) {
         cudaGetLastError();
         per = 1;
@@ -349,17 +419,32 @@ static int occ_of() {
     return per;
 }
 
-static int batched_occupancy(int threads, int ppt) {
-    if (threads == 64) return ppt == 1 ? occ_of<64, 1>() : occ_of<64, 2>();
-    if (threads == 256) return ppt == 1 ? occ_of<256, 1>() : occ_of<256, 2>();
-    return ppt == 1 ? occ_of<128, 1>() : occ_of<128, 2>();
+template <int MODE>
+static int occ_mode(int threads, int ppt) {
+    if (threads == 64) return ppt == 1 ? occ_of<64, 1, MODE>() : occ_of<64, 2, MODE>();
+    if (threads == 256) return ppt == 1 ? occ_of<256, 1, MODE>() : occ_of<256, 2, MODE>();
+    return ppt == 1 ? occ_of<128, 1, MODE>() : occ_of<128, 2, MODE>();
+}
+
+static int batched_occupancy(int threads, int ppt, int mode) {
+    return mode == 2 ? occ_mode<2>(threads, ppt) : occ_mode<1>(threads, ppt);
+}
+
+// Tiles [t0, t1) with walk MODE; the persistent grid never exceeds the tile count.
+template <int BLOCK, int PPT, int MODE>
+static void launch_batched_mode(lj_ctx* ctx, lj_batch* b, const float* p4, float* energy, float* force, int t0,
+                                int t1) {
+    if (t1 <= t0) return;
+    const int grid = std::min(b->persistent_blocks[MODE - 1], t1 - t0);
+    k_pair_batched<BLOCK, PPT, MODE><<<grid, BLOCK, 0, ctx->stream>>>(
+        b->d_sys, reinterpret_cast<const float4*>(p4), b->soa, b->soa_ld, b->cell, b->offsets, b->d_tiles + t0,
+        t1 - t0, b->d_counter + (MODE - 1), energy, force, b->te, b->tw, b->tnp, ctx->d_status);
 }
 
 template <int BLOCK, int PPT>
 static void launch_batched_pair(lj_ctx* ctx, lj_batch* b, const float* p4, float* energy, float* force) {
-    k_pair_batched<BLOCK, PPT><<<b->persistent_blocks, BLOCK, 0, ctx->stream>>>(
-        b->d_sys, reinterpret_cast<const float4*>(p4), b->cell, b->offsets, b->ntotal, b->d_tiles, b->ntiles,
-        b->d_counter, energy, force, b->te, b->tw, b->tnp, ctx->d_status);
+    launch_batched_mode<BLOCK, PPT, 2>(ctx, b, p4, energy, force, b->ntiles1, b->ntiles);
+    launch_batched_mode<BLOCK, PPT, 1>(ctx, b, p4, energy, force, 0, b->ntiles1);
 }
 
 // The batched step on ctx->stream (no synchronisation, no allocation once the
@@ -383,7 +468,14 @@ static lj_status batch_step(lj_ctx* ctx, lj_batch* b, const float* x, const floa
     if ((st = bin_finish(ctx, b->total_cells, n, x, y, z, 1, LJ_ORDER_X, b->counts, b->offsets, nullptr,
                          index ? &sorted : nullptr, xyzi, b->cell)) != LJ_OK)
         return st;
-    if (cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), s) != cudaSuccess) return LJ_ECUDA;
+    if (b->any_soa && n > 0) {
+        long long blocks = ((long long)n + 255) / 256;
+        if (blocks > (long long)ctx->sm_count * 8) blocks = (long long)ctx->sm_count * 8;
+        k_split_soa_batched<<<(int)blocks, 256, 0, s>>>(b->d_sys, b->d_firsts, b->nsys, b->xyzi, n, b->soa_ld,
+                                                        b->soa);
+        if ((st = last_launch_status()) != LJ_OK) return st;
+    }
+    if (cudaMemsetAsync(b->d_counter, 0, 2 * sizeof(unsigned), s) != cudaSuccess) return LJ_ECUDA;
     const int T = b->cfg.threads, P = b->cfg.per_thread;
     if (T == 64)
         P == 1 ? launch_batched_pair<64, 1>(ctx, b, xyzi, energy, force)

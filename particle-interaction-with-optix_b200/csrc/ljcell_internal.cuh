@@ -99,6 +99,8 @@ struct lj_ctx {
     lj_tuning tuning;            // implementation choices (lj_set_tuning)
     void* tiles;                 // tile counter, tile count and cell-block tiles of the pair kernel
     size_t tiles_bytes;
+    void* soa;                   // x, y, z arrays of the sorted particles for the SoA pair kernel
+    size_t soa_bytes;
     // end-to-end buffers (lj_simulate_host): device buffers, a second stream for the device-to-host
     // copies and the events that order it after the pair chunks
     void* e2e;
@@ -117,6 +119,8 @@ lj_status bin_prepare(lj_ctx* ctx, int n, long long nc, int* counts);
 lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const float* y, const float* z, int stride,
                      lj_order order, int* counts, int* offsets, lj_cell_desc* cells, lj_particles* sorted,
                      float* sorted_xyzi, int* sorted_cell);
+// Default pair kernel (lj_tuning numbering) for n particles binned in g with LJ_ORDER_X (pair.cu).
+int default_pair_kernel(int n, const lj_grid& g);
 // Pair stage of lj_compute over the sorted targets [kb, ke) (pair.cu); totals cover those targets only.
 lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm, int n, const float* xyzi,
                              const int* cs, const int* off, lj_order order, float* energy, float* force,

@@ -25,7 +25,15 @@
 
 namespace ljc {
 
-constexpr double kDenseCell = 32.0;  // particles per cell above which the default is the register-window kernel
+constexpr double kDenseCell = 32.0;  // particles per cell from which the default reads neighbours as SoA pairs
+
+// Default pair kernel for LJ_ORDER_X (measured on B200): the packed row passes, reading neighbours from
+// the float4 records on sparse grids and from SoA copies of x, y, z on dense ones, where the windows are
+// long and the copy is paid back.
+int default_pair_kernel(int n, const lj_grid& g) {
+    const double per_cell = (double)n / ((double)g.dim[0] * g.dim[1] * g.dim[2]);
+    return per_cell >= kDenseCell ? 7 : 6;
+}
 
 template <bool XWIN>
 __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairParams pp, const float4* __restrict__ p,
@@ -119,16 +127,14 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
     pp.slack = grid_slack(*g);
     if (order == LJ_ORDER_X) {
         int kernel = ctx->tuning.pair_kernel;
-        if (kernel == 0) {
-            // default: dense grids (many particles per cell, long windows) run best with the windows in
-            // registers, sparse ones with the windows in shared memory (measured on B200)
-            const double per_cell = (double)n / ((double)g->dim[0] * g->dim[1] * g->dim[2]);
-            kernel = per_cell >= kDenseCell ? 2 : 1;
-        }
+        if (kernel == 0) kernel = default_pair_kernel(n, *g);
         switch (kernel) {
             case 4:  // cell-block tiles cover whole target ranges only; a sub-range runs kernel 1
                 if (kb == 0 && ke == n) return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
                 break;
+            case 7: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 2, energy, force, totals, kb, ke);
+            case 6: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 1, energy, force, totals, kb, ke);
+            case 5: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 0, energy, force, totals, kb, ke);
             case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);
             case 2: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals, kb, ke);
             default: break;  // 1: windows in shared memory (below)
@@ -191,7 +197,9 @@ extern "C" lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj
     int best = 1;
     float bt = 3.4e38f;
     lj_status st = LJ_OK;
-    for (int k = 1; k <= 3 && st == LJ_OK; ++k) {
+    static const int kCandidates[] = {1, 2, 3, 5, 6, 7};
+    for (int ki = 0; ki < 6 && st == LJ_OK; ++ki) {
+        const int k = kCandidates[ki];
         ctx->tuning.pair_kernel = k;
         float ms = 3.4e38f;
         for (int r = 0; r < 3 && st == LJ_OK; ++r) {  // the first run warms up

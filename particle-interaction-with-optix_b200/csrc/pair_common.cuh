@@ -224,6 +224,9 @@ float grid_slack(const lj_grid& g);
 lj_status launch_pair_direct(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                              const int* cs, const int* off, bool compact, float* energy, float* force,
                              lj_totals* totals, int kb, int ke);
+lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
+                           const int* cs, const int* off, int mode, float* energy, float* force,
+                           lj_totals* totals, int kb, int ke);
 lj_status launch_pair_tiled(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                             const int* off, float* energy, float* force, lj_totals* totals);
 

@@ -1,0 +1,93 @@
+// pair_pass.cu -- single-system kernel of the warp-synchronous row passes
+// (the walk itself is in pair_pass.cuh).
+#include "pair_pass.cuh"
+
+namespace ljc {
+
+namespace {
+constexpr int kPassThreads = 128;
+}  // namespace
+
+// One thread per target of [kb, ke).  MODE as pass_target.
+template <int MODE>
+__global__ void __launch_bounds__(kPassThreads) k_pair_pass(GridDev g, PairParams pp, const float4* __restrict__ p,
+                                                            const float* __restrict__ sx,
+                                                            const float* __restrict__ sy,
+                                                            const float* __restrict__ sz,
+                                                            const int* __restrict__ cs, const int* __restrict__ off,
+                                                            int n, int kb, int ke, float* __restrict__ energy,
+                                                            float* __restrict__ force, Partial* part,
+                                                            unsigned* counter, lj_totals* totals, unsigned* status) {
+    const int k = kb + blockIdx.x * kPassThreads + threadIdx.x;
+    const bool active = k < ke;
+    int c = 0;
+    if (active) {
+        c = __ldg(&cs[k]);
+        if (c < 0 || c >= g.gx * g.gy * g.gz) {
+            atomicOr(status, kFlagRange);
+            c = 0;
+        }
+    }
+    PassAcc a;
+    pass_target<MODE>(g, pp, p, reinterpret_cast<const float2*>(sx), reinterpret_cast<const float2*>(sy),
+                      reinterpret_cast<const float2*>(sz), off, 0, n, k, c, active, a);
+    const float ea = a.e.x + a.e.y, wa = a.w.x + a.w.y;
+    if (active) {
+        if (energy) energy[k] = pp.e4 * ea;
+        if (force) {
+            const float nf = -pp.fscale;
+            force[3 * (size_t)k + 0] = nf * (a.fx.x + a.fx.y);
+            force[3 * (size_t)k + 1] = nf * (a.fy.x + a.fy.y);
+            force[3 * (size_t)k + 2] = nf * (a.fz.x + a.fz.y);
+        }
+    }
+    reduce_totals<kPassThreads>(0.5 * (double)pp.e4 * (double)ea, 0.5 * (double)pp.e24 * (double)wa,
+                                (unsigned long long)a.np, part, counter, totals);
+}
+
+__global__ void __launch_bounds__(256) k_split_soa(const float4* __restrict__ p, int n, int ld, float* __restrict__ s) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + 2; i += gridDim.x * blockDim.x) {
+        const float4 q = i < n ? p[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        s[i] = q.x;
+        s[ld + i] = q.y;
+        s[2 * (size_t)ld + i] = q.z;
+    }
+}
+
+lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
+                           const int* cs, const int* off, int mode, float* energy, float* force,
+                           lj_totals* totals, int kb, int ke) {
+    const int blocks = (ke - kb + kPassThreads - 1) / kPassThreads;
+    const size_t need = 256 + (size_t)blocks * sizeof(Partial);
+    if (need > ctx->red_bytes) {
+        lj_status s = grow(&ctx->red, &ctx->red_bytes, need);
+        if (s != LJ_OK) return s;
+        if (cudaMemsetAsync(ctx->red, 0, 256, ctx->stream) != cudaSuccess) return LJ_ECUDA;
+    }
+    unsigned* counter = static_cast<unsigned*>(ctx->red);
+    Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
+    const float4* p4 = reinterpret_cast<const float4*>(xyzi);
+    const GridDev gd = to_dev(*g);
+    if (mode == 2) {
+        const int ld = (n + 2 + 63) & ~63;
+        lj_status s = grow(&ctx->soa, &ctx->soa_bytes, 3 * (size_t)ld * sizeof(float));
+        if (s != LJ_OK) return s;
+        float* sx = static_cast<float*>(ctx->soa);
+        // the SoA copy is made once per pass over all targets (the first target range starts at 0)
+        if (kb == 0) k_split_soa<<<min((n + 2 + 255) / 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(p4, n, ld, sx);
+        k_pair_pass<2><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, sx, sx + ld, sx + 2 * (size_t)ld, cs,
+                                                                 off, n, kb, ke, energy, force, part, counter,
+                                                                 totals, ctx->d_status);
+    } else if (mode == 1) {
+        k_pair_pass<1><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, nullptr, nullptr, nullptr, cs, off, n,
+                                                                 kb, ke, energy, force, part, counter, totals,
+                                                                 ctx->d_status);
+    } else {
+        k_pair_pass<0><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, nullptr, nullptr, nullptr, cs, off, n,
+                                                                 kb, ke, energy, force, part, counter, totals,
+                                                                 ctx->d_status);
+    }
+    return last_launch_status();
+}
+
+}  // namespace ljc
