@@ -213,6 +213,7 @@ struct lj_batch {
     std::vector<lj_grid> grids;
     long long total_cells = 0;
     ljc::SysDev* d_sys = nullptr;
+    ljc::BinSys* d_binsys = nullptr;  // grids and cell bases for the within-cell sort
     int* d_firsts = nullptr;
     int4* d_tiles = nullptr;
     int ntiles = 0;
@@ -244,6 +245,7 @@ namespace ljc {
 
 static void free_plan_buffers(lj_batch* b) {
     cudaFree(b->d_sys);
+    cudaFree(b->d_binsys);
     cudaFree(b->d_firsts);
     cudaFree(b->d_tiles);
     cudaFree(b->d_counter);
@@ -258,6 +260,7 @@ static void free_plan_buffers(lj_batch* b) {
     b->soa = nullptr;
     b->soa_ld = 0;
     b->d_sys = nullptr;
+    b->d_binsys = nullptr;
     b->d_firsts = nullptr;
     b->d_tiles = nullptr;
     b->d_counter = nullptr;
@@ -366,6 +369,7 @@ static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
             (st = dev_alloc(&b->te, N)) != LJ_OK || (st = dev_alloc(&b->tw, N)) != LJ_OK ||
             (st = dev_alloc(&b->tnp, N)) != LJ_OK || (st = dev_alloc(&b->d_sys, (size_t)b->nsys)) != LJ_OK ||
             (st = dev_alloc(&b->d_firsts, (size_t)b->nsys)) != LJ_OK ||
+            (st = dev_alloc(&b->d_binsys, (size_t)b->nsys)) != LJ_OK ||
             (st = dev_alloc(&b->d_counter, (size_t)64)) != LJ_OK)
             return st;
     }
@@ -389,9 +393,14 @@ static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
         b->tiles_cap = tiles.size();
     }
     std::vector<int> firsts(b->nsys);
-    for (int s = 0; s < b->nsys; ++s) firsts[s] = b->sys[s].first;
+    std::vector<BinSys> binsys(b->nsys);
+    for (int s = 0; s < b->nsys; ++s) {
+        firsts[s] = b->sys[s].first;
+        binsys[s] = BinSys{b->sd[s].g, b->sd[s].cell_base, b->sd[s].first};
+    }
     if (cudaMemcpy(b->d_sys, b->sd.data(), sizeof(SysDev) * b->nsys, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(b->d_firsts, firsts.data(), sizeof(int) * b->nsys, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->d_binsys, binsys.data(), sizeof(BinSys) * b->nsys, cudaMemcpyHostToDevice) != cudaSuccess ||
         (!tiles.empty() && cudaMemcpy(b->d_tiles, tiles.data(), sizeof(int4) * tiles.size(),
                                       cudaMemcpyHostToDevice) != cudaSuccess))
         return LJ_ECUDA;
@@ -466,7 +475,8 @@ static lj_status batch_step(lj_ctx* ctx, lj_batch* b, const float* x, const floa
     sorted.index = index;
     float* xyzi = reinterpret_cast<float*>(b->xyzi);
     if ((st = bin_finish(ctx, b->total_cells, n, x, y, z, 1, LJ_ORDER_X, b->counts, b->offsets, nullptr,
-                         index ? &sorted : nullptr, xyzi, b->cell)) != LJ_OK)
+                         index ? &sorted : nullptr, xyzi, b->cell, GridDev{}, b->d_binsys, b->d_firsts, b->nsys)) !=
+        LJ_OK)
         return st;
     if (b->any_soa && n > 0) {
         long long blocks = ((long long)n + 255) / 256;

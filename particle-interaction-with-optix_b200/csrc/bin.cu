@@ -6,12 +6,13 @@
 //   PrefixFullV2 (prefixsum.hpp:160-215)           -> k_scan    (single-pass
 //        decoupled look-back exclusive scan; no recursion, no allocation, no
 //        host synchronisation)
-//   InitNewCells (cudaLJ.cu:428-439)               -> k_descriptors / folded into k_cell_sort
-//   MoveParticlesToNewCells (cudaLJ.cu:441-471)    -> k_scatter + k_cell_sort
+//   InitNewCells (cudaLJ.cu:428-439)               -> k_descriptors
+//   MoveParticlesToNewCells (cudaLJ.cu:441-471)    -> k_scatter + k_cell_rank (+ k_large_sort)
 //        (ticket scatter, then a per-cell sort that makes the order a pure
 //        function of the input, repacking positions as float4 x, y, z, index)
 // and ComputeNbInteractions (cudaLJ.cu:255-297) -> k_candidates (per cell
 // instead of per particle).
+#include <algorithm>
 #include <climits>
 #include <mutex>
 
@@ -24,7 +25,7 @@ namespace ljc {
 // cell elect a leader (__match_any_sync) which adds the group's size with one
 // atomic; each lane's ticket is the leader's old value plus its rank in the
 // group.  Tickets give a slot inside the cell; their order is not
-// deterministic, which k_cell_sort fixes.
+// deterministic, which k_cell_rank fixes.
 template <bool TICKETS>
 __global__ void __launch_bounds__(256) k_count(GridDev g, const float* __restrict__ x, const float* __restrict__ y,
                                                const float* __restrict__ z, int stride, int n,
@@ -204,18 +205,40 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const int* __restrict__ c
 // Moves each particle to offsets[cell] + ticket as float4 (x, y, z, index
 // bits).  The slot is range-checked so that a corrupted offsets array cannot
 // write out of bounds.
+// Four particles per thread per round, all loads issued before the stores: the kernel is bound by
+// the latency of the offset gather and of the scattered 16-byte writes, not by bandwidth.
 __global__ void __launch_bounds__(256) k_scatter(const float* __restrict__ x, const float* __restrict__ y,
                                                  const float* __restrict__ z, int stride, int n,
                                                  const int2* __restrict__ ct, const int* __restrict__ offsets,
                                                  float4* __restrict__ tmp, unsigned* status) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int2 c = ct[i];
-        const long long slot = (long long)__ldg(&offsets[c.x]) + c.y;
-        if (slot >= 0 && slot < n)
-            tmp[slot] = make_float4(x[i * stride], y[i * stride], z[i * stride], __int_as_float((int)i));
-        else
-            atomicOr(status, kFlagRange);
+    constexpr int U = 4;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * step) {
+        int2 c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long i = i0 + u * step;
+            c[u] = i < n ? __ldg(&ct[i]) : make_int2(0, 0);
+        }
+        long long slot[U];
+        float px[U], py[U], pz[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long i = i0 + u * step;
+            slot[u] = i < n ? (long long)__ldg(&offsets[c[u].x]) + c[u].y : -1;
+            px[u] = i < n ? __ldg(&x[i * stride]) : 0.f;
+            py[u] = i < n ? __ldg(&y[i * stride]) : 0.f;
+            pz[u] = i < n ? __ldg(&z[i * stride]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long i = i0 + u * step;
+            if (i >= n) continue;
+            if (slot[u] >= 0 && slot[u] < n)
+                tmp[slot[u]] = make_float4(px[u], py[u], pz[u], __int_as_float((int)i));
+            else
+                atomicOr(status, kFlagRange);
+        }
     }
 }
 
@@ -247,76 +270,69 @@ __device__ __forceinline__ void emit(const SortOut& o, long long slot, float4 r,
     if (o.sidx) o.sidx[slot] = __float_as_int(r.w);
 }
 
-constexpr int kWarpSortMax = 2048;
-constexpr int kLargeCap = 4096;  // cells beyond the warp sort, per step
+constexpr int kRankMax = 512;    // cells up to this size are ranked record by record
+constexpr int kLargeCapMin = 4096;
 
-// One warp per group of 32 consecutive cells.  Lanes read the group's offsets
-// (coalesced), write the CellDescriptor view, copy singleton cells directly,
-// and then sort every cell of 2..kWarpSortMax particles cooperatively by
-// ranking (each record's rank = number of smaller keys in its cell).  Larger
-// cells go to a list handled by k_large_sort.
+// One thread per record of the scattered (cell-grouped, unordered within a cell) array.  The
+// record's cell is recomputed from its position with the count kernel's formula (the same float
+// operations on the same values, so the same cell; with several systems, the system is found from
+// the record's original index); its rank is the number of records of the same cell with a smaller
+// key (a loop over the cell's records, which the neighbouring threads read too: L1 hits), and it
+// is written at offset + rank.  Every lane is busy whatever the cell sizes.  Cells above kRankMax
+// go to a list handled by k_large_sort (registered by the thread of the cell's first slot).
 template <int ORDER>
-__global__ void __launch_bounds__(256) k_cell_sort(const float4* __restrict__ tmp, const int* __restrict__ offsets,
-                                                   long long ncells, int n, SortOut so, lj_cell_desc* cells,
+__global__ void __launch_bounds__(256) k_cell_rank(const float4* __restrict__ tmp, const int* __restrict__ offsets,
+                                                   GridDev g, const BinSys* __restrict__ sys,
+                                                   const int* __restrict__ firsts, int nsys, int n, SortOut so,
                                                    int* large, int large_cap, unsigned* status) {
-    const int lane = threadIdx.x & 31;
-    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long g0 = gwarp * 32; g0 < ncells; g0 += nwarps * 32) {
-        const long long c = g0 + lane;
-        const bool in = c < ncells;
-        int o0 = in ? __ldg(&offsets[c]) : 0;
-        const int onext = __shfl_down_sync(0xffffffffu, o0, 1);
-        int o1 = (lane < 31 && c + 1 < ncells) ? onext : (in ? __ldg(&offsets[c + 1]) : 0);
-        o0 = min(max(o0, 0), n);
-        o1 = min(max(o1, o0), n);
-        const int cnt = in ? o1 - o0 : 0;
-        if (cells && in) cells[c] = lj_cell_desc{cnt, o0};
-        if (cnt == 1) emit(so, o0, tmp[o0], (int)c);
-        if (cnt > kWarpSortMax) {
-            const int slot = atomicAdd(&large[0], 1);
-            if (slot < large_cap)
-                large[1 + slot] = (int)c;
-            else
-                atomicOr(status, kFlagRange);
-        }
-        unsigned multi = __ballot_sync(0xffffffffu, cnt > 1 && cnt <= kWarpSortMax);
-        while (multi) {
-            const int src = __ffs(multi) - 1;
-            multi &= multi - 1;
-            const int base = __shfl_sync(0xffffffffu, o0, src);
-            const int m = __shfl_sync(0xffffffffu, cnt, src);
-            const int cell = (int)(g0 + src);
-            if (m <= 32) {
-                const float4 r = lane < m ? tmp[base + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-                const float rx = r.x;
-                const int ri = __float_as_int(r.w);
-                int rank = 0;
-                for (int q = 0; q < m; ++q) {
-                    const float qx = __shfl_sync(0xffffffffu, rx, q);
-                    const int qi = __shfl_sync(0xffffffffu, ri, q);
-                    rank += key_less<ORDER>(qx, qi, rx, ri) ? 1 : 0;
-                }
-                if (lane < m) emit(so, (long long)base + rank, r, cell);
-            } else {
-                for (int b = 0; b < m; b += 32) {
-                    const int e = b + lane;
-                    const bool ok = e < m;
-                    const float4 r = ok ? tmp[base + e] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    const int ri = __float_as_int(r.w);
-                    int rank = 0;
-                    for (int q = 0; q < m; ++q) {
-                        const float4 t = tmp[base + q];  // warp-uniform address: one broadcast load
-                        rank += key_less<ORDER>(t.x, __float_as_int(t.w), r.x, ri) ? 1 : 0;
-                    }
-                    if (ok) emit(so, (long long)base + rank, r, cell);
-                }
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const float4 r = tmp[s];
+        int c;
+        if (nsys == 0) {
+            c = cell_of(g, r.x, r.y, r.z);
+        } else {
+            const int i = __float_as_int(r.w);
+            int lo = 0, hi = nsys - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(&firsts[mid]) <= i)
+                    lo = mid;
+                else
+                    hi = mid - 1;
             }
+            c = sys[lo].cell_base + cell_of(sys[lo].g, r.x, r.y, r.z);
         }
+        so.out_cell[s] = c;  // every slot of a cell holds its id, whatever the order inside the cell
+        const int o0 = min(max(__ldg(&offsets[c]), 0), n);
+        const int o1 = min(max(__ldg(&offsets[c + 1]), o0), n);
+        const int m = o1 - o0;
+        if (m > kRankMax) {
+            if (s == o0) {
+                const int slot = atomicAdd(&large[0], 1);
+                if (slot < large_cap)
+                    large[1 + slot] = c;
+                else
+                    atomicOr(status, kFlagRange);
+            }
+            continue;
+        }
+        const float rx = r.x;
+        const int ri = __float_as_int(r.w);
+        int rank = 0;
+        for (int j = o0; j < o1; ++j) {
+            const float4 t = tmp[j];
+            rank += key_less<ORDER>(t.x, __float_as_int(t.w), rx, ri) ? 1 : 0;
+        }
+        const long long slot = (long long)o0 + rank;
+        so.out4[slot] = r;
+        if (so.sx) so.sx[slot] = r.x;
+        if (so.sy) so.sy[slot] = r.y;
+        if (so.sz) so.sz[slot] = r.z;
+        if (so.sidx) so.sidx[slot] = __float_as_int(r.w);
     }
 }
 
-// Cells larger than kWarpSortMax (rare: clustered or degenerate inputs): one
+// Cells larger than kRankMax (rare: clustered or degenerate inputs): one
 // CTA per cell sorts 2048-record chunks in shared memory (bitonic network),
 // then merges runs pairwise, each record finding its place in the partner run
 // by binary search; ping-pong between the cell's tmp and out ranges.
@@ -519,12 +535,13 @@ lj_status bin_prepare(lj_ctx* ctx, int n, long long nc, int* counts) {
         ctx->tmp4 = static_cast<float4*>(p2);
         ctx->part_cap = need;
     }
-    if (!ctx->large_cells) {
-        void* p = nullptr;
-        size_t cap = 0;
-        if ((s = grow(&p, &cap, sizeof(int) * (1 + kLargeCap))) != LJ_OK) return s;
+    const size_t large_need = (size_t)std::max<long long>(kLargeCapMin, (long long)n / kRankMax + 1);
+    if (!ctx->large_cells || ctx->large_cap < large_need) {
+        void* p = ctx->large_cells;
+        size_t cap = ctx->large_cells ? sizeof(int) * (1 + ctx->large_cap) : 0;
+        if ((s = grow(&p, &cap, sizeof(int) * (1 + large_need))) != LJ_OK) return s;
         ctx->large_cells = static_cast<int*>(p);
-        ctx->large_cap = kLargeCap;
+        ctx->large_cap = large_need;
     }
     if (cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, ctx->stream) != cudaSuccess) return LJ_ECUDA;
     if (cudaMemsetAsync(ctx->large_cells, 0, sizeof(int), ctx->stream) != cudaSuccess) return LJ_ECUDA;
@@ -535,7 +552,8 @@ lj_status bin_prepare(lj_ctx* ctx, int n, long long nc, int* counts) {
 // scatter, within-cell sort (with the descriptor view and SoA outputs).
 lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const float* y, const float* z, int stride,
                      lj_order order, int* counts, int* offsets, lj_cell_desc* cells, lj_particles* sorted,
-                     float* sorted_xyzi, int* sorted_cell) {
+                     float* sorted_xyzi, int* sorted_cell, const GridDev& g, const BinSys* sys, const int* firsts,
+                     int nsys) {
     lj_status s;
     cudaStream_t st = ctx->stream;
     if ((s = launch_scan(ctx, counts, nc, offsets)) != LJ_OK) return s;
@@ -551,19 +569,26 @@ lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const flo
         so.sz = sorted->z;
         so.sidx = sorted->index;
     }
-    const int sort_blocks = grid_for(ctx, (nc + 31) / 32, 8, 16);
-    if (order == LJ_ORDER_X) {
-        k_cell_sort<LJ_ORDER_X><<<sort_blocks, 256, 0, st>>>(ctx->tmp4, offsets, nc, n, so, cells, ctx->large_cells,
-                                                            kLargeCap, ctx->d_status);
+    const int lcap = (int)ctx->large_cap;
+    if (n > 0) {
+        if (order == LJ_ORDER_X) {
+            k_cell_rank<LJ_ORDER_X><<<grid_for(ctx, n, 256), 256, 0, st>>>(ctx->tmp4, offsets, g, sys, firsts, nsys, n,
+                                                                           so, ctx->large_cells, lcap, ctx->d_status);
+            if ((s = last_launch_status()) != LJ_OK) return s;
+            k_large_sort<LJ_ORDER_X><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so, ctx->large_cells,
+                                                                     lcap);
+        } else {
+            k_cell_rank<LJ_ORDER_INDEX><<<grid_for(ctx, n, 256), 256, 0, st>>>(ctx->tmp4, offsets, g, sys, firsts, nsys,
+                                                                               n, so, ctx->large_cells, lcap,
+                                                                               ctx->d_status);
+            if ((s = last_launch_status()) != LJ_OK) return s;
+            k_large_sort<LJ_ORDER_INDEX><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so,
+                                                                         ctx->large_cells, lcap);
+        }
         if ((s = last_launch_status()) != LJ_OK) return s;
-        k_large_sort<LJ_ORDER_X><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so, ctx->large_cells,
-                                                                 kLargeCap);
-    } else {
-        k_cell_sort<LJ_ORDER_INDEX><<<sort_blocks, 256, 0, st>>>(ctx->tmp4, offsets, nc, n, so, cells,
-                                                                ctx->large_cells, kLargeCap, ctx->d_status);
-        if ((s = last_launch_status()) != LJ_OK) return s;
-        k_large_sort<LJ_ORDER_INDEX><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so, ctx->large_cells,
-                                                                     kLargeCap);
+    }
+    if (cells) {
+        k_descriptors<<<grid_for(ctx, nc, 256), 256, 0, st>>>(offsets, nc, cells);
     }
     return last_launch_status();
 }
@@ -586,7 +611,8 @@ extern "C" lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x
                                                                       ctx->cell_ticket, ctx->d_status);
         if ((s = last_launch_status()) != LJ_OK) return s;
     }
-    return bin_finish(ctx, nc, n, x, y, z, stride, order, counts, offsets, cells, sorted, sorted_xyzi, sorted_cell);
+    return bin_finish(ctx, nc, n, x, y, z, stride, order, counts, offsets, cells, sorted, sorted_xyzi, sorted_cell,
+                      to_dev(*g), nullptr, nullptr, 0);
 }
 
 extern "C" lj_status lj_count_candidates(lj_ctx* ctx, const lj_grid* g, const int* offsets,

@@ -116,9 +116,17 @@ lj_status grow(void** p, size_t* cap, size_t need);
 lj_status last_launch_status();
 // Cell-grid build stages (bin.cu), shared by lj_bin and the batched step.
 lj_status bin_prepare(lj_ctx* ctx, int n, long long nc, int* counts);
+// The within-cell sort recomputes each record's cell: from grid g when nsys == 0, else from the
+// system table (sys[s] for the last s with firsts[s] <= the record's original index).
+struct BinSys {
+    GridDev g;
+    int cell_base;
+    int first;
+};
 lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const float* y, const float* z, int stride,
                      lj_order order, int* counts, int* offsets, lj_cell_desc* cells, lj_particles* sorted,
-                     float* sorted_xyzi, int* sorted_cell);
+                     float* sorted_xyzi, int* sorted_cell, const GridDev& g, const BinSys* sys, const int* firsts,
+                     int nsys);
 // Default pair kernel (lj_tuning numbering) for n particles binned in g with LJ_ORDER_X (pair.cu).
 int default_pair_kernel(int n, const lj_grid& g);
 // Pair stage of lj_compute over the sorted targets [kb, ke) (pair.cu); totals cover those targets only.
