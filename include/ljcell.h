@@ -334,6 +334,20 @@ LJ_API lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params
  * lj_sync returns LJ_ETIMEOUT and the context stays usable.  ncells > 4096. */
 LJ_API lj_status lj_test_scan_withheld_tile(lj_ctx* ctx, const int* counts, long long ncells, int* offsets);
 
+/* ------------------------------------------------------------- spatial sort
+ * Replaces reorder(N, points, radius) (SDK/optixMultiSphereAABB/sort.cu:29-41,
+ * key kernel count_per_cell :7-18): sorts n float4 points in place by the key
+ * of their cell and stores the key in .w as float.  width = int(1.0f/radius);
+ * key = int(x/radius) + int(y/radius)*width + int(z/radius)*width*width with
+ * IEEE float division, truncation and int arithmetic, as the reference.
+ * Points with equal .w keep their input order (the reference's thrust::sort
+ * leaves that order unspecified).  points: device, 16-byte aligned.  The
+ * domain is the reference's, coordinates in [0, 1]: a point whose key falls
+ * outside it (or a NaN coordinate) is reported as LJ_ERANGE by lj_sync and
+ * sorted as key 0.  width <= 512 (radius > 1/513), else LJ_EUNSUPPORTED.
+ * Scratch is the context's; asynchronous on its stream. */
+LJ_API lj_status lj_reorder(lj_ctx* ctx, int n, float* points, float radius);
+
 /* ------------------------------------------------------------- end to end
  * One call with HOST buffers, the shape of executeSimulation's step
  * (cudaLJ.cu:613-653) without the generation: copies positions to the device,

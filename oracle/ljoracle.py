@@ -380,3 +380,27 @@ def mixed_forces(g: Grid, b: Binned, uy, uz, rc: float, eps: float = 1.0, sigma:
     sl = slice(k0, k1)
     return ConfigResult(None, None, e64[sl], f64[sl], int(pairs.value), float(etot.value), float(vir.value), es[sl],
                         fs[sl], nnb[sl])
+
+
+# --------------------------------------------------------------------- spatial sort
+def reorder(points: np.ndarray, radius: float) -> np.ndarray:
+    """Restatement of the reference's reorder(N, points, radius)
+    (SDK/optixMultiSphereAABB/sort.cu:29-41) and its key kernel count_per_cell
+    (sort.cu:7-18): width = int(1.0f / radius) (:30); per point
+    cell = int(x / radius) per axis in float32 IEEE division and truncation
+    (:12-14); id = cell_x + cell_y * width + cell_z * width * width in int
+    (:15); .w = float(id) (:16); sort by .w ascending (:20-25, :38).  Points
+    of equal .w keep their input order (a stable sort): the reference's
+    thrust::sort leaves that order unspecified, so comparisons against the
+    reference itself use per-key sets.  Returns a new (n, 4) float32 array."""
+    p = np.ascontiguousarray(points, dtype=np.float32)
+    r = np.float32(radius)
+    width = int(np.float32(1.0) / r)
+    q = p[:, :3] / r
+    c = np.trunc(q).astype(np.int64)
+    ident = c[:, 0] + c[:, 1] * width + c[:, 2] * width * width
+    w = ident.astype(np.int32).astype(np.float32)
+    order = np.argsort(w, kind="stable")
+    out = p[order].copy()
+    out[:, 3] = w[order]
+    return out

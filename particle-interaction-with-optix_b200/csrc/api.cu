@@ -110,6 +110,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->tiles);
     cudaFree(c->e2e);
     cudaFree(c->soa);
+    cudaFree(c->reorder);
     if (c->e2e_ready) {
         cudaStreamSynchronize(c->copy_stream);
         for (int i = 0; i < 8; ++i) cudaEventDestroy(c->e2e_ev[i]);
@@ -126,7 +127,7 @@ extern "C" lj_status lj_set_stream(lj_ctx* c, void* stream) {
 }
 
 extern "C" lj_status lj_set_tuning(lj_ctx* c, const lj_tuning* t) {
-    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 7) return LJ_EINVAL;
+    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 11) return LJ_EINVAL;
     c->tuning = *t;
     return LJ_OK;
 }

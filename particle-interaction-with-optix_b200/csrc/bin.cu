@@ -719,3 +719,139 @@ extern "C" lj_status lj_exclusive_scan_noalloc(const int* counts, long long ncel
     k_noalloc_mark<<<1, 1, 0, st>>>(status, offsets, ncells);
     return last_launch_status();
 }
+
+// ---------------------------------------------------------------- spatial sort (lj_reorder)
+// The operation of the reference's reorder() (SDK/optixMultiSphereAABB/sort.cu:29-41 with its key
+// kernel count_per_cell, :7-18): each float4 point gets the key of its cell, width = int(1 / radius),
+// id = int(x / radius) + int(y / radius) * width + int(z / radius) * width^2 (IEEE division,
+// truncation, int arithmetic), stored in .w as float, and the points are sorted by .w.  Here the sort
+// is a counting sort over the keys on the binning kernels: count with tickets, scan, ticket scatter
+// (k_scatter, reading x, y, z with stride 4), then a rank by original index within each key, so
+// points of equal .w keep their input order (the reference's thrust::sort leaves that order open).
+// Keys are counted as int(float(id)), the value .w holds, so two ids that round to the same float
+// share a bin exactly as they compare equal in the reference.
+namespace ljc {
+
+constexpr int kReorderMaxWidth = 512;  // int(1 / radius) <= 512: at most 134,480,385 keys
+
+struct ReorderKey {
+    float radius;
+    int width;
+    int nkeys;
+};
+
+__device__ __forceinline__ int reorder_key(const ReorderKey& rk, float x, float y, float z, bool& bad) {
+    const int cx = __float2int_rz(__fdiv_rn(x, rk.radius));
+    const int cy = __float2int_rz(__fdiv_rn(y, rk.radius));
+    const int cz = __float2int_rz(__fdiv_rn(z, rk.radius));
+    const long long id = (long long)cx + (long long)cy * rk.width + (long long)cz * rk.width * rk.width;
+    bad = !(x == x && y == y && z == z) || id < 0 || id > INT_MAX;
+    const int kf = bad ? 0 : __float2int_rz(__int2float_rn((int)id));
+    if (kf >= rk.nkeys) {
+        bad = true;
+        return 0;
+    }
+    return kf;
+}
+
+__global__ void __launch_bounds__(256) k_reorder_count(const float4* __restrict__ pts, int n, ReorderKey rk,
+                                                       int* __restrict__ counts, int2* __restrict__ ct,
+                                                       unsigned* status) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = pts[i];
+        bool bad;
+        const int key = reorder_key(rk, p.x, p.y, p.z, bad);
+        if (bad) atomicOr(status, kFlagRange);
+        // one atomic per distinct key in the warp (points of a key often arrive together)
+        const unsigned peers = __match_any_sync(__activemask(), key);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if ((int)lane_id() == leader) base = atomicAdd(&counts[key], __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        ct[i] = make_int2(key, base + __popc(peers & lanemask_lt()));
+    }
+}
+
+// Rank of each scattered record among the records of its key, by original index (as k_cell_rank);
+// keys above kRankMax records go to the large list for k_large_sort<LJ_ORDER_INDEX>.
+__global__ void __launch_bounds__(256) k_reorder_rank(const float4* __restrict__ tmp, const int2* __restrict__ ct,
+                                                      const int* __restrict__ offsets, int n, SortOut so, int* large,
+                                                      int large_cap, unsigned* status) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const float4 r = tmp[s];
+        const int i = __float_as_int(r.w);
+        const int c = (i >= 0 && i < n) ? __ldg(&ct[i]).x : 0;
+        so.out_cell[s] = c;
+        const int o0 = min(max(__ldg(&offsets[c]), 0), n);
+        const int o1 = min(max(__ldg(&offsets[c + 1]), o0), n);
+        const int m = o1 - o0;
+        if (m > kRankMax) {
+            if (s == o0) {
+                const int slot = atomicAdd(&large[0], 1);
+                if (slot < large_cap)
+                    large[1 + slot] = c;
+                else
+                    atomicOr(status, kFlagRange);
+            }
+            continue;
+        }
+        int rank = 0;
+        for (int j = o0; j < o1; ++j) rank += __float_as_int(tmp[j].w) < i ? 1 : 0;
+        so.out4[(long long)o0 + rank] = r;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_reorder_emit(const float4* __restrict__ sorted, const int* __restrict__ key,
+                                                      int n, float4* __restrict__ pts) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const float4 r = sorted[s];
+        pts[s] = make_float4(r.x, r.y, r.z, __int2float_rn(key[s]));
+    }
+}
+
+}  // namespace ljc
+
+extern "C" lj_status lj_reorder(lj_ctx* ctx, int n, float* points, float radius) {
+    if (!ctx || n < 0 || (n > 0 && !points) || !(radius > 0.0f) || !(radius < 3.4e38f)) return LJ_EINVAL;
+    if (reinterpret_cast<uintptr_t>(points) & 15) return LJ_EINVAL;
+    if (n == 0) return LJ_OK;
+    const float wf = 1.0f / radius;
+    if (!(wf < (float)kReorderMaxWidth + 1.0f)) return LJ_EUNSUPPORTED;
+    const long long width = (long long)wf;  // the reference's int(1.0f / radius)
+    // coordinates in [0, 1] give cell coordinates in [0, width]
+    const long long max_id = width + width * width + width * width * width;
+    const long long max_key = std::max(max_id, (long long)(float)max_id);
+    const long long nkeys = max_key + 1;
+    ReorderKey rk{radius, (int)width, (int)nkeys};
+    lj_status s;
+    // scratch: counts[nkeys], offsets[nkeys + 1] (16-byte aligned), sorted float4[n], keys int[n]
+    const size_t cnt_bytes = ((size_t)nkeys * sizeof(int) + 255) & ~(size_t)255;
+    const size_t off_bytes = (((size_t)nkeys + 1) * sizeof(int) + 255) & ~(size_t)255;
+    const size_t rec_bytes = (size_t)n * sizeof(float4);
+    const size_t key_bytes = (size_t)n * sizeof(int);
+    if ((s = grow(&ctx->reorder, &ctx->reorder_bytes, cnt_bytes + off_bytes + rec_bytes + key_bytes)) != LJ_OK)
+        return s;
+    char* base = static_cast<char*>(ctx->reorder);
+    int* counts = reinterpret_cast<int*>(base);
+    int* offsets = reinterpret_cast<int*>(base + cnt_bytes);
+    float4* sorted = reinterpret_cast<float4*>(base + cnt_bytes + off_bytes);
+    int* keys = reinterpret_cast<int*>(base + cnt_bytes + off_bytes + rec_bytes);
+    cudaStream_t st = ctx->stream;
+    if ((s = bin_prepare(ctx, n, nkeys, counts)) != LJ_OK) return s;  // tickets, tmp4, large list; counts zeroed
+    const float4* p4 = reinterpret_cast<const float4*>(points);
+    k_reorder_count<<<grid_for(ctx, n, 256), 256, 0, st>>>(p4, n, rk, counts, ctx->cell_ticket, ctx->d_status);
+    if ((s = last_launch_status()) != LJ_OK) return s;
+    if ((s = launch_scan(ctx, counts, nkeys, offsets)) != LJ_OK) return s;
+    k_scatter<<<grid_for(ctx, n, 256), 256, 0, st>>>(points, points + 1, points + 2, 4, n, ctx->cell_ticket, offsets,
+                                                     ctx->tmp4, ctx->d_status);
+    if ((s = last_launch_status()) != LJ_OK) return s;
+    SortOut so{sorted, keys, nullptr, nullptr, nullptr, nullptr};
+    const int lcap = (int)ctx->large_cap;
+    k_reorder_rank<<<grid_for(ctx, n, 256), 256, 0, st>>>(ctx->tmp4, ctx->cell_ticket, offsets, n, so,
+                                                          ctx->large_cells, lcap, ctx->d_status);
+    if ((s = last_launch_status()) != LJ_OK) return s;
+    k_large_sort<LJ_ORDER_INDEX><<<ctx->sm_count, 1024, 0, st>>>(ctx->tmp4, offsets, n, so, ctx->large_cells, lcap);
+    if ((s = last_launch_status()) != LJ_OK) return s;
+    k_reorder_emit<<<grid_for(ctx, n, 256), 256, 0, st>>>(sorted, keys, n, reinterpret_cast<float4*>(points));
+    return last_launch_status();
+}

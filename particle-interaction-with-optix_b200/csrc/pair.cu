@@ -133,6 +133,10 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
                 if (kb == 0 && ke == n) return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
                 break;
             case 7: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 2, energy, force, totals, kb, ke);
+            case 8: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 3, energy, force, totals, kb, ke);
+            case 9: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 4, energy, force, totals, kb, ke);
+            case 10: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 5, energy, force, totals, kb, ke);
+            case 11: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 6, energy, force, totals, kb, ke);
             case 6: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 1, energy, force, totals, kb, ke);
             case 5: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 0, energy, force, totals, kb, ke);
             case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);

@@ -316,6 +316,148 @@ __global__ void __launch_bounds__(kMixThreads) k_pair_mixed_reg(GridDev g, MixPa
                                (unsigned long long)np, part, counter, totals);
 }
 
+// ---------------------------------------------------------------- row passes
+// The mixed records walked as the plain default walks its float4 records (pair_pass.cuh): the 9 rows
+// in 5 warp-synchronous passes (own row; then opposite rows paired), two candidates per step in the
+// paired FP32 instructions, each half rounding as the scalar kernels above, so the distance test and
+// the pair count are those of k_pair_mixed.  Each candidate takes the target frame of its row.  Sums:
+// per pass two FP32 partials (even and odd steps), added to the running (sum, compensation) pairs with
+// TwoSum when the pass ends.
+
+struct MixPassAcc {
+    float se, ce, sx, cx, sy, cy, sz, cz;  // compensated sums
+    float2 w;                              // virial partials (the totals reduce in FP64)
+    unsigned np;
+};
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// One pass: window A = [sA, sA + LA) of row ra, then window B = [offB + LA, offB + L) of row rb.
+template <bool OWN>
+__device__ __forceinline__ void mix_walk_pass(const float2* __restrict__ rec, int k, float xi, float2 ui, int ra,
+                                              int sA, int LA, int rb, int offB, int L, const MixParams& mp,
+                                              MixPassAcc& a) {
+    const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
+    const float ntyA = (float)(ra % 3 - 1) - ui.x, ntzA = (float)(ra / 3 - 1) - ui.y;
+    const float ntyB = (float)(rb % 3 - 1) - ui.x, ntzB = (float)(rb / 3 - 1) - ui.y;
+    const float2 nxi = f2(-xi, -xi), invw = f2(mp.invw, mp.invw), nsig2 = f2(-mp.sig2u, -mp.sig2u),
+                 two = f2(2.0f, 2.0f);
+    const float rc2 = mp.rc2u;
+    float2 pe = f2(0.f, 0.f), px = pe, py = pe, pz = pe;
+    for (int v = 0; v < maxL; v += 2) {
+        const int v1 = v + 1;
+        const bool ok0 = v < L, ok1 = v1 < L;
+        const bool a0 = v < LA, a1 = v1 < LA;
+        const int j0 = v + (a0 ? sA : offB);
+        const int j1 = v1 + (a1 ? sA : offB);
+        const float2 q0 = __ldg(&rec[ok0 ? j0 : k]);
+        const float2 q1 = __ldg(&rec[ok1 ? j1 : k]);
+        bool m0 = ok0, m1 = ok1;
+        if (OWN) {
+            m0 = m0 && j0 != k;
+            m1 = m1 && j1 != k;
+        }
+        const float2 u0 = unpack_yz(q0.y), u1 = unpack_yz(q1.y);
+        const float2 dx = __fmul2_rn(__fadd2_rn(f2(q0.x, q1.x), nxi), invw);
+        const float2 dy = __fadd2_rn(f2(u0.x, u1.x), f2(a0 ? ntyA : ntyB, a1 ? ntyA : ntyB));
+        const float2 dz = __fadd2_rn(f2(u0.y, u1.y), f2(a0 ? ntzA : ntzB, a1 ? ntzA : ntzB));
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const bool in0 = m0 && r2.x < rc2, in1 = m1 && r2.y < rc2;
+        const float2 ir2 = f2(in0 ? rcp_approx(r2.x) : 0.f, in1 ? rcp_approx(r2.y) : 0.f);
+        const float2 s2n = __fmul2_rn(nsig2, ir2);
+        const float2 s4 = __fmul2_rn(s2n, s2n);
+        const float2 ns6 = __fmul2_rn(s4, s2n);
+        const float2 s12 = __fmul2_rn(ns6, ns6);
+        pe = __fadd2_rn(pe, __fadd2_rn(s12, ns6));
+        const float2 t = __ffma2_rn(two, s12, ns6);
+        a.w = __fadd2_rn(a.w, t);
+        const float2 fsn = __fmul2_rn(t, s2n);  // minus the force sums, as in pair_pass.cuh
+        px = __ffma2_rn(fsn, dx, px);
+        py = __ffma2_rn(fsn, dy, py);
+        pz = __ffma2_rn(fsn, dz, pz);
+        a.np += (unsigned)in0 + (unsigned)in1;
+    }
+    two_sum_add(a.se, a.ce, pe.x);
+    two_sum_add(a.se, a.ce, pe.y);
+    two_sum_add(a.sx, a.cx, -px.x);
+    two_sum_add(a.sx, a.cx, -px.y);
+    two_sum_add(a.sy, a.cy, -py.x);
+    two_sum_add(a.sy, a.cy, -py.y);
+    two_sum_add(a.sz, a.cz, -pz.x);
+    two_sum_add(a.sz, a.cz, -pz.y);
+}
+
+__global__ void __launch_bounds__(kMixThreads) k_pair_mixed_pass(GridDev g, MixParams mp,
+                                                                 const float2* __restrict__ rec,
+                                                                 const int* __restrict__ cs,
+                                                                 const int* __restrict__ off, int n,
+                                                                 float* __restrict__ energy, float* __restrict__ force,
+                                                                 Partial* part, unsigned* counter, lj_totals* totals,
+                                                                 unsigned* status) {
+    const int k = blockIdx.x * kMixThreads + threadIdx.x;
+    const bool active = k < n;
+    int ws[9], wl[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) ws[r] = wl[r] = 0;
+    float xi = 0.f;
+    float2 ui = f2(0.f, 0.f);
+    if (active) {
+        const float2 ri = __ldg(&rec[k]);
+        xi = ri.x;
+        ui = unpack_yz(ri.y);
+        int c = __ldg(&cs[k]);
+        if (c < 0 || c >= g.gx * g.gy * g.gz) {
+            atomicOr(status, kFlagRange);
+            c = 0;
+        }
+        int cx, cy, cz;
+        decode_cell(g, c, cx, cy, cz);
+        const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
+        const float slack = mp.slack + 8.0f * FLT_EPSILON * fabsf(xi);
+        // the windows of k_pair_mixed_reg
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+            const int dz = r / 3 - 1, dy = r % 3 - 1;
+            const int z = cz + dz, y = cy + dy;
+            if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) continue;
+            float dzm = dz < 0 ? ui.y : (dz > 0 ? 1.0f - ui.y : 0.f);
+            float dym = dy < 0 ? ui.x : (dy > 0 ? 1.0f - ui.x : 0.f);
+            dzm = fmaxf(dzm - 1e-5f, 0.f);
+            dym = fmaxf(dym - 1e-5f, 0.f);
+            const float d2 = fmaf(dym, dym, dzm * dzm);
+            if (d2 >= mp.rc2uw) continue;
+            const int rb = (z * g.gy + y) * g.gx;
+            const int s = min(max(__ldg(&off[rb + xl]), 0), n);
+            const int e = min(max(__ldg(&off[rb + xh + 1]), s), n);
+            const float h = sqrtf(mp.rc2uw - d2) * mp.w + slack;
+            const int lo = lower_rx(rec, s, e, xi - h);
+            const int hi = upper_rx(rec, lo, e, xi + h);
+            ws[r] = lo;
+            wl[r] = hi - lo;
+        }
+    }
+    MixPassAcc a;
+    a.se = a.ce = a.sx = a.cx = a.sy = a.cy = a.sz = a.cz = 0.f;
+    a.w = f2(0.f, 0.f);
+    a.np = 0;
+    mix_walk_pass<true>(rec, k, xi, ui, 4, ws[4], wl[4], 4, 0, wl[4], mp, a);
+    mix_walk_pass<false>(rec, k, xi, ui, 3, ws[3], wl[3], 5, ws[5] - wl[3], wl[3] + wl[5], mp, a);
+    mix_walk_pass<false>(rec, k, xi, ui, 1, ws[1], wl[1], 7, ws[7] - wl[1], wl[1] + wl[7], mp, a);
+    mix_walk_pass<false>(rec, k, xi, ui, 0, ws[0], wl[0], 8, ws[8] - wl[0], wl[0] + wl[8], mp, a);
+    mix_walk_pass<false>(rec, k, xi, ui, 2, ws[2], wl[2], 6, ws[6] - wl[2], wl[2] + wl[6], mp, a);
+    if (active) {
+        if (energy) energy[k] = mp.e4 * (a.se + a.ce);
+        if (force) {
+            force[3 * (size_t)k + 0] = mp.fscale * (a.sx + a.cx);
+            force[3 * (size_t)k + 1] = mp.fscale * (a.sy + a.cy);
+            force[3 * (size_t)k + 2] = mp.fscale * (a.sz + a.cz);
+        }
+    }
+    reduce_totals<kMixThreads>(0.5 * (double)mp.e4 * ((double)a.se + (double)a.ce),
+                               0.5 * (double)mp.e24 * ((double)a.w.x + (double)a.w.y), (unsigned long long)a.np,
+                               part, counter, totals);
+}
+
 }  // namespace ljc
 
 using namespace ljc;
@@ -365,9 +507,14 @@ extern "C" lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_pa
     }
     unsigned* counter = static_cast<unsigned*>(ctx->red);
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
-    // windows in shared memory unless pair_kernel 2 asks for registers (measured faster for the mixed
-    // records on sparse and dense grids alike)
-    if (ctx->tuning.pair_kernel == 2)
+    // row passes unless pair_kernel 1 (windows in shared memory) or 2 (windows in registers) asks for a
+    // flat walk
+    if (ctx->tuning.pair_kernel != 1 && ctx->tuning.pair_kernel != 2)
+        k_pair_mixed_pass<<<blocks, kMixThreads, 0, ctx->stream>>>(to_dev(*g), mp,
+                                                                   reinterpret_cast<const float2*>(rec), sorted_cell,
+                                                                   offsets, n, energy, force, part, counter, totals,
+                                                                   ctx->d_status);
+    else if (ctx->tuning.pair_kernel == 2)
         k_pair_mixed_reg<<<blocks, kMixThreads, 0, ctx->stream>>>(to_dev(*g), mp, reinterpret_cast<const float2*>(rec),
                                                                   sorted_cell, offsets, n, energy, force, part,
                                                                   counter, totals, ctx->d_status);

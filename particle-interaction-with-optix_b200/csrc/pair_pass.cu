@@ -78,14 +78,18 @@ lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, 
         k_pair_pass<2><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, sx, sx + ld, sx + 2 * (size_t)ld, cs,
                                                                  off, n, kb, ke, energy, force, part, counter,
                                                                  totals, ctx->d_status);
-    } else if (mode == 1) {
-        k_pair_pass<1><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, nullptr, nullptr, nullptr, cs, off, n,
-                                                                 kb, ke, energy, force, part, counter, totals,
-                                                                 ctx->d_status);
     } else {
-        k_pair_pass<0><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, nullptr, nullptr, nullptr, cs, off, n,
-                                                                 kb, ke, energy, force, part, counter, totals,
-                                                                 ctx->d_status);
+        auto kern = k_pair_pass<0>;
+        switch (mode) {
+            case 1: kern = k_pair_pass<1>; break;
+            case 3: kern = k_pair_pass<3>; break;
+            case 4: kern = k_pair_pass<4>; break;
+            case 5: kern = k_pair_pass<5>; break;
+            case 6: kern = k_pair_pass<6>; break;
+            default: break;
+        }
+        kern<<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, nullptr, nullptr, nullptr, cs, off, n, kb, ke,
+                                                       energy, force, part, counter, totals, ctx->d_status);
     }
     return last_launch_status();
 }

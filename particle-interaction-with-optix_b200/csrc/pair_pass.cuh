@@ -38,8 +38,23 @@ struct PassAcc {
     unsigned np;
 };
 
+// Non-blocking hint that brings the 128-byte line holding *ptr into L1 (no register is written, so the
+// warp does not wait for it).
+__device__ __forceinline__ void prefetch_l1(const void* ptr) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(ptr));
+}
+
+// Hints for the first lines of window [s, s + L) of float4 records (8 records per line).
+__device__ __forceinline__ void prefetch_window(const float4* __restrict__ p, int s, int L) {
+    if (L > 0) prefetch_l1(p + s);
+    if (L > 8) prefetch_l1(p + s + 8);
+    if (L > 16) prefetch_l1(p + s + 16);
+}
+
 // One pass: window A = [sA, sA + LA), then window B = [offB + LA, offB + L).  OWN: skip j == k.
-template <bool PACKED, bool OWN>
+// CLAMP: a lane past the end of its windows loads its own record (index k) instead of skipping the
+// load, so no default value has to be kept in registers; the masks discard it either way.
+template <bool PACKED, bool OWN, bool CLAMP = false>
 __device__ __forceinline__ void walk_pass(const float4* __restrict__ p, int k, const float4& pi, int sA, int LA,
                                           int offB, int L, float rc2, float sig2, PassAcc& a) {
     const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
@@ -52,9 +67,16 @@ __device__ __forceinline__ void walk_pass(const float4* __restrict__ p, int k, c
             const bool ok0 = v < L, ok1 = v1 < L;
             const int j0 = v + (v < LA ? sA : offB);
             const int j1 = v1 + (v1 < LA ? sA : offB);
-            float4 q0 = pi, q1 = pi;
-            if (ok0) q0 = __ldg(&p[j0]);
-            if (ok1) q1 = __ldg(&p[j1]);
+            float4 q0, q1;
+            if (CLAMP) {
+                q0 = __ldg(&p[ok0 ? j0 : k]);
+                q1 = __ldg(&p[ok1 ? j1 : k]);
+            } else {
+                q0 = pi;
+                q1 = pi;
+                if (ok0) q0 = __ldg(&p[j0]);
+                if (ok1) q1 = __ldg(&p[j1]);
+            }
             bool m0 = ok0, m1 = ok1;
             if (OWN) {
                 m0 = m0 && j0 != k;
@@ -198,9 +220,63 @@ __device__ __forceinline__ void pass_windows(const GridDev& g, const PairParams&
     }
 }
 
+// As pass_windows, in two phases: first every row's cell range [s, e) is read and L1 hints are issued
+// for all of its lines (the ranges of the 32 targets of a warp overlap, so the hints of a warp cover a
+// few dozen distinct lines), then the binary searches run.  The searches and the walk then find the
+// rows in L1 instead of waiting for each first touch in turn.
+__device__ __forceinline__ void pass_windows_pf(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
+                                                const int* __restrict__ off, int obase, int n, const float4& pi, int c,
+                                                int (&ws)[9], int (&wl)[9]) {
+    int cx, cy, cz;
+    decode_cell(g, c, cx, cy, cz);
+    const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
+    const float slack = pp.slack + 8.0f * FLT_EPSILON * fmaxf(fabsf(pi.x), fmaxf(fabsf(pi.y), fabsf(pi.z)));
+    float hs[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        const int dz = r / 3 - 1, dy = r % 3 - 1;
+        const int z = cz + dz, y = cy + dy;
+        hs[r] = -1.f;
+        if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) continue;
+        float dzm = 0.f, dym = 0.f;
+        if (dz < 0) dzm = pi.z - fmaf((float)cz, g.w, g.oz);
+        if (dz > 0) dzm = fmaf((float)(cz + 1), g.w, g.oz) - pi.z;
+        if (dy < 0) dym = pi.y - fmaf((float)cy, g.w, g.oy);
+        if (dy > 0) dym = fmaf((float)(cy + 1), g.w, g.oy) - pi.y;
+        dzm = fmaxf(dzm - slack, 0.f);
+        dym = fmaxf(dym - slack, 0.f);
+        const float d2 = fmaf(dym, dym, dzm * dzm);
+        if (d2 >= pp.rc2w) continue;
+        const int rb = (z * g.gy + y) * g.gx;
+        const int s = min(max(__ldg(&off[rb + xl]) - obase, 0), n);
+        const int e = min(max(__ldg(&off[rb + xh + 1]) - obase, s), n);
+        ws[r] = s;
+        wl[r] = e;
+        hs[r] = sqrtf(pp.rc2w - d2) + slack;
+    }
+#pragma unroll
+    for (int r = 0; r < 9; ++r)
+        if (hs[r] >= 0.f)
+            for (int q = ws[r] & ~7; q < wl[r]; q += 8) prefetch_l1(p + q);
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        if (hs[r] < 0.f) {
+            ws[r] = wl[r] = 0;
+            continue;
+        }
+        const int s = lower_x(p, ws[r], wl[r], pi.x - hs[r]);
+        const int e = upper_x(p, s, wl[r], pi.x + hs[r]);
+        ws[r] = s;
+        wl[r] = e - s;
+    }
+}
+
 // Per-target pass walk.  Every lane of the warp must call it (inactive lanes with active = false):
 // the passes' loop bounds are warp maxima.  MODE 0: scalar, float4 neighbours; 1: packed, float4
-// neighbours; 2: packed, SoA neighbours x2 / y2 / z2 (pairs of the local arrays, even-aligned).
+// neighbours; 2: packed, SoA neighbours x2 / y2 / z2 (pairs of the local arrays, even-aligned);
+// 3: as 1 with clamped loads and L1 hints for the next pass's windows issued before each pass;
+// 4: as 1 with the hints only; 5: as 1 with clamped loads only; 6: as 5, with every stencil row's
+// lines hinted into L1 before the window searches (pass_windows_pf).
 // Indices k, and those of p / x2 / y2 / z2, are local: [0, n).
 template <int MODE>
 __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
@@ -213,7 +289,10 @@ __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& 
     float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (active) {
         pi = __ldg(&p[k]);
-        pass_windows(g, pp, p, off, obase, n, pi, c, ws, wl);
+        if (MODE == 6)
+            pass_windows_pf(g, pp, p, off, obase, n, pi, c, ws, wl);
+        else
+            pass_windows(g, pp, p, off, obase, n, pi, c, ws, wl);
     }
     a.e = a.w = a.fx = a.fy = a.fz = make_float2(0.f, 0.f);
     a.np = 0;
@@ -225,12 +304,30 @@ __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& 
         walk_pass_soa<false>(x2, y2, z2, k, pi, ws[0], ws[0] + wl[0], ws[8], ws[8] + wl[8], rc2, sig2, a);
         walk_pass_soa<false>(x2, y2, z2, k, pi, ws[2], ws[2] + wl[2], ws[6], ws[6] + wl[6], rc2, sig2, a);
     } else {
-        constexpr bool PACKED = MODE == 1;
-        walk_pass<PACKED, true>(p, k, pi, ws[4], wl[4], 0, wl[4], rc2, sig2, a);
-        walk_pass<PACKED, false>(p, k, pi, ws[3], wl[3], ws[5] - wl[3], wl[3] + wl[5], rc2, sig2, a);
-        walk_pass<PACKED, false>(p, k, pi, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
-        walk_pass<PACKED, false>(p, k, pi, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
-        walk_pass<PACKED, false>(p, k, pi, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
+        constexpr bool PACKED = MODE != 0;
+        constexpr bool CL = MODE == 3 || MODE == 5 || MODE == 6;
+        constexpr bool PF = MODE == 3 || MODE == 4;
+        if (PF) {
+            prefetch_window(p, ws[3], wl[3]);
+            prefetch_window(p, ws[5], wl[5]);
+        }
+        walk_pass<PACKED, true, CL>(p, k, pi, ws[4], wl[4], 0, wl[4], rc2, sig2, a);
+        if (PF) {
+            prefetch_window(p, ws[1], wl[1]);
+            prefetch_window(p, ws[7], wl[7]);
+        }
+        walk_pass<PACKED, false, CL>(p, k, pi, ws[3], wl[3], ws[5] - wl[3], wl[3] + wl[5], rc2, sig2, a);
+        if (PF) {
+            prefetch_window(p, ws[0], wl[0]);
+            prefetch_window(p, ws[8], wl[8]);
+        }
+        walk_pass<PACKED, false, CL>(p, k, pi, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
+        if (PF) {
+            prefetch_window(p, ws[2], wl[2]);
+            prefetch_window(p, ws[6], wl[6]);
+        }
+        walk_pass<PACKED, false, CL>(p, k, pi, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
+        walk_pass<PACKED, false, CL>(p, k, pi, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
     }
 }
 

@@ -124,6 +124,7 @@ def _load() -> C.CDLL:
         "lj_pack_mixed": (i32, [vp, C.POINTER(Grid), i32, vp, vp, vp]),
         "lj_compute_mixed": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp]),
         "lj_test_scan_withheld_tile": (i32, [vp, vp, i64, vp]),
+        "lj_reorder": (i32, [vp, i32, vp, C.c_float]),
         "lj_simulate_host": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
                                    C.POINTER(Totals)]),
     }
@@ -141,7 +142,7 @@ ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj
                "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_autotune_compute", "lj_batch_create",
                "lj_batch_destroy", "lj_batch_get_config", "lj_batch_grid", "lj_batch_run", "lj_batch_run_graph",
                "lj_batch_run_separate", "lj_batch_autotune", "lj_pack_mixed", "lj_compute_mixed",
-               "lj_test_scan_withheld_tile", "lj_simulate_host")
+               "lj_test_scan_withheld_tile", "lj_reorder", "lj_simulate_host")
 
 
 def lib() -> C.CDLL:
@@ -386,6 +387,13 @@ class Context:
         _check(_lib.lj_compute_mixed(self._h, C.byref(g), C.byref(p), b.n, _ptr(rec), _ptr(b.cell), _ptr(b.offsets),
                                      _ptr(energy), _ptr(force), _ptr(totals)), "lj_compute_mixed")
         return energy, force, totals
+
+    def reorder(self, points, radius: float):
+        """lj_reorder: sorts the (n, 4) float32 device tensor `points` in place by cell key (stored in
+        column 3), as the reference's reorder(N, points, radius)."""
+        n = int(points.shape[0]) if points.numel() else 0
+        _check(_lib.lj_reorder(self._h, n, _ptr(points), C.c_float(radius)), "lj_reorder")
+        return points
 
     def simulate_host(self, g: Grid, p: Params, hx: np.ndarray, hy: np.ndarray, hz: np.ndarray,
                       energy: np.ndarray | None = None, force: np.ndarray | None = None,
