@@ -220,7 +220,7 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  * whose launch shape is fixed at 128 threads per particle, cudaLJ.cu:519-520).
  * Results do not depend on them except in the last bits of floating-point
  * sums.  pair_kernel, for particles binned with LJ_ORDER_X:
- *   0 = default: 7 when the grid averages 32 or more particles per cell, else 6,
+ *   0 = default: 9 when the grid averages 2 or more particles per cell, else 6,
  *   1 = direct: one thread per target, neighbours through L1, its windows
  *       in shared memory,
  *   2 = direct with the windows in registers,
@@ -232,9 +232,13 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  *       (opposite rows paired), coalesced neighbour loads, no divergence,
  *   6 = row passes with two candidates per step in paired FP32 instructions,
  *   7 = as 6, neighbours read from SoA copies of x, y, z in even-aligned
- *       pairs (one 8-byte load per coordinate pair; the copy is made per call).
+ *       pairs (one 8-byte load per coordinate pair; the copy is made per call),
+ *   8 = row passes with two consecutive targets per lane: their windows
+ *       merged, each candidate loaded once and tested against both targets
+ *       in one paired FP32 evaluation,
+ *   9 = as 8 with the registers capped at 64 per thread (higher occupancy).
  * With a non-finite coordinate (reported as LJ_ERANGE) the outputs of the
- * particles whose windows hold it are unspecified under 5-7. */
+ * particles whose windows hold it are unspecified under 5-9. */
 typedef struct {
     int pair_kernel;
     int reserved[7];

@@ -301,7 +301,7 @@ static lj_status build_grids(lj_batch* b) {
         d.cell_base = (int)base;
         d.first = y.first;
         d.n = y.n;
-        d.walk = default_pair_kernel(y.n, g) == 7 ? 2 : 1;
+        d.walk = dense_grid(y.n, g) ? 2 : 1;
         d.soa_base = (int)soa;
         soa += ((long long)y.n + 2 + 1) & ~1LL;
         if (d.walk == 2) b->any_soa = true;
@@ -554,10 +554,27 @@ static lj_status batch_graph(lj_ctx* ctx, lj_batch* b, const float* x, const flo
     return LJ_OK;
 }
 
-// One plain lj_bin + lj_compute per system (the path the batched step replaces).
+// One plain lj_bin + lj_compute per system (the path the batched step replaces), each with the
+// single-system kernel of the walk the batched kernel takes for it (6: float4 neighbours, 7: SoA pairs),
+// so per-particle results are equal bit for bit.
+static lj_status batch_separate_one(lj_ctx* ctx, lj_batch* b, int s, const float* x, const float* y, const float* z,
+                                    float* energy, float* force, int* index, lj_totals* totals);
+
 static lj_status batch_separate(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
                                 float* energy, float* force, int* index, lj_totals* totals) {
-    for (int s = 0; s < b->nsys; ++s) {
+    const lj_tuning saved = ctx->tuning;
+    lj_status st = LJ_OK;
+    for (int s = 0; s < b->nsys && st == LJ_OK; ++s) {
+        ctx->tuning.pair_kernel = b->sd[s].walk == 2 ? 7 : 6;
+        st = batch_separate_one(ctx, b, s, x, y, z, energy, force, index, totals);
+    }
+    ctx->tuning = saved;
+    return st;
+}
+
+static lj_status batch_separate_one(lj_ctx* ctx, lj_batch* b, int s, const float* x, const float* y, const float* z,
+                                    float* energy, float* force, int* index, lj_totals* totals) {
+    {
         const lj_system& sy = b->sys[s];
         const SysDev& d = b->sd[s];
         const int f = sy.first;

@@ -333,8 +333,9 @@ struct MixPassAcc {
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 // One pass: window A = [sA, sA + LA) of row ra, then window B = [offB + LA, offB + L) of row rb.
+// kl: index loaded by a lane past the end of its windows (valid; the masks discard it).
 template <bool OWN>
-__device__ __forceinline__ void mix_walk_pass(const float2* __restrict__ rec, int k, float xi, float2 ui, int ra,
+__device__ __forceinline__ void mix_walk_pass(const float2* __restrict__ rec, int k, int kl, float xi, float2 ui, int ra,
                                               int sA, int LA, int rb, int offB, int L, const MixParams& mp,
                                               MixPassAcc& a) {
     const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
@@ -350,8 +351,8 @@ __device__ __forceinline__ void mix_walk_pass(const float2* __restrict__ rec, in
         const bool a0 = v < LA, a1 = v1 < LA;
         const int j0 = v + (a0 ? sA : offB);
         const int j1 = v1 + (a1 ? sA : offB);
-        const float2 q0 = __ldg(&rec[ok0 ? j0 : k]);
-        const float2 q1 = __ldg(&rec[ok1 ? j1 : k]);
+        const float2 q0 = __ldg(&rec[ok0 ? j0 : kl]);
+        const float2 q1 = __ldg(&rec[ok1 ? j1 : kl]);
         bool m0 = ok0, m1 = ok1;
         if (OWN) {
             m0 = m0 && j0 != k;
@@ -436,15 +437,16 @@ __global__ void __launch_bounds__(kMixThreads) k_pair_mixed_pass(GridDev g, MixP
             wl[r] = hi - lo;
         }
     }
+    const int kl = min(k, n - 1);
     MixPassAcc a;
     a.se = a.ce = a.sx = a.cx = a.sy = a.cy = a.sz = a.cz = 0.f;
     a.w = f2(0.f, 0.f);
     a.np = 0;
-    mix_walk_pass<true>(rec, k, xi, ui, 4, ws[4], wl[4], 4, 0, wl[4], mp, a);
-    mix_walk_pass<false>(rec, k, xi, ui, 3, ws[3], wl[3], 5, ws[5] - wl[3], wl[3] + wl[5], mp, a);
-    mix_walk_pass<false>(rec, k, xi, ui, 1, ws[1], wl[1], 7, ws[7] - wl[1], wl[1] + wl[7], mp, a);
-    mix_walk_pass<false>(rec, k, xi, ui, 0, ws[0], wl[0], 8, ws[8] - wl[0], wl[0] + wl[8], mp, a);
-    mix_walk_pass<false>(rec, k, xi, ui, 2, ws[2], wl[2], 6, ws[6] - wl[2], wl[2] + wl[6], mp, a);
+    mix_walk_pass<true>(rec, k, kl, xi, ui, 4, ws[4], wl[4], 4, 0, wl[4], mp, a);
+    mix_walk_pass<false>(rec, k, kl, xi, ui, 3, ws[3], wl[3], 5, ws[5] - wl[3], wl[3] + wl[5], mp, a);
+    mix_walk_pass<false>(rec, k, kl, xi, ui, 1, ws[1], wl[1], 7, ws[7] - wl[1], wl[1] + wl[7], mp, a);
+    mix_walk_pass<false>(rec, k, kl, xi, ui, 0, ws[0], wl[0], 8, ws[8] - wl[0], wl[0] + wl[8], mp, a);
+    mix_walk_pass<false>(rec, k, kl, xi, ui, 2, ws[2], wl[2], 6, ws[6] - wl[2], wl[2] + wl[6], mp, a);
     if (active) {
         if (energy) energy[k] = mp.e4 * (a.se + a.ce);
         if (force) {

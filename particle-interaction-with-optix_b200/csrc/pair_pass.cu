@@ -45,6 +45,55 @@ __global__ void __launch_bounds__(kPassThreads) k_pair_pass(GridDev g, PairParam
                                 (unsigned long long)a.np, part, counter, totals);
 }
 
+// Two targets per thread (pass_target2): thread t of the launch takes targets kb + 2t and kb + 2t + 1.
+template <int MINB>
+__global__ void __launch_bounds__(kPassThreads, MINB) k_pair_pass2(GridDev g, PairParams pp, const float4* __restrict__ p,
+                                                             const int* __restrict__ cs, const int* __restrict__ off,
+                                                             int n, int kb, int ke, float* __restrict__ energy,
+                                                             float* __restrict__ force, Partial* part,
+                                                             unsigned* counter, lj_totals* totals, unsigned* status) {
+    const int ka = kb + 2 * (blockIdx.x * kPassThreads + threadIdx.x);
+    const bool activeA = ka < ke, activeB = ka + 1 < ke;
+    const int ncell = g.gx * g.gy * g.gz;
+    int ca = 0, cb = 0;
+    if (activeA) {
+        ca = __ldg(&cs[ka]);
+        if (ca < 0 || ca >= ncell) {
+            atomicOr(status, kFlagRange);
+            ca = 0;
+        }
+    }
+    if (activeB) {
+        cb = __ldg(&cs[ka + 1]);
+        if (cb < 0 || cb >= ncell) {
+            atomicOr(status, kFlagRange);
+            cb = 0;
+        }
+    }
+    Pass2Acc a;
+    pass_target2(g, pp, p, off, 0, n, ka, ca, cb, activeA, activeB, a);
+    const float nf = -pp.fscale;
+    if (activeA) {
+        if (energy) energy[ka] = pp.e4 * a.e.x;
+        if (force) {
+            force[3 * (size_t)ka + 0] = nf * a.fx.x;
+            force[3 * (size_t)ka + 1] = nf * a.fy.x;
+            force[3 * (size_t)ka + 2] = nf * a.fz.x;
+        }
+    }
+    if (activeB) {
+        if (energy) energy[ka + 1] = pp.e4 * a.e.y;
+        if (force) {
+            force[3 * (size_t)ka + 3] = nf * a.fx.y;
+            force[3 * (size_t)ka + 4] = nf * a.fy.y;
+            force[3 * (size_t)ka + 5] = nf * a.fz.y;
+        }
+    }
+    reduce_totals<kPassThreads>(0.5 * (double)pp.e4 * ((double)a.e.x + (double)a.e.y),
+                                0.5 * (double)pp.e24 * ((double)a.w.x + (double)a.w.y), (unsigned long long)a.np, part,
+                                counter, totals);
+}
+
 __global__ void __launch_bounds__(256) k_split_soa(const float4* __restrict__ p, int n, int ld, float* __restrict__ s) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + 2; i += gridDim.x * blockDim.x) {
         const float4 q = i < n ? p[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -57,7 +106,8 @@ __global__ void __launch_bounds__(256) k_split_soa(const float4* __restrict__ p,
 lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                            const int* cs, const int* off, int mode, float* energy, float* force,
                            lj_totals* totals, int kb, int ke) {
-    const int blocks = (ke - kb + kPassThreads - 1) / kPassThreads;
+    const int per_block = mode >= 3 ? 2 * kPassThreads : kPassThreads;
+    const int blocks = (ke - kb + per_block - 1) / per_block;
     const size_t need = 256 + (size_t)blocks * sizeof(Partial);
     if (need > ctx->red_bytes) {
         lj_status s = grow(&ctx->red, &ctx->red_bytes, need);
@@ -68,7 +118,13 @@ lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, 
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
     const float4* p4 = reinterpret_cast<const float4*>(xyzi);
     const GridDev gd = to_dev(*g);
-    if (mode == 2) {
+    if (mode == 3) {
+        k_pair_pass2<1><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force,
+                                                                  part, counter, totals, ctx->d_status);
+    } else if (mode == 4) {
+        k_pair_pass2<8><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force,
+                                                                  part, counter, totals, ctx->d_status);
+    } else if (mode == 2) {
         const int ld = (n + 2 + 63) & ~63;
         lj_status s = grow(&ctx->soa, &ctx->soa_bytes, 3 * (size_t)ld * sizeof(float));
         if (s != LJ_OK) return s;
@@ -79,15 +135,7 @@ lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, 
                                                                  off, n, kb, ke, energy, force, part, counter,
                                                                  totals, ctx->d_status);
     } else {
-        auto kern = k_pair_pass<0>;
-        switch (mode) {
-            case 1: kern = k_pair_pass<1>; break;
-            case 3: kern = k_pair_pass<3>; break;
-            case 4: kern = k_pair_pass<4>; break;
-            case 5: kern = k_pair_pass<5>; break;
-            case 6: kern = k_pair_pass<6>; break;
-            default: break;
-        }
+        auto kern = mode == 1 ? k_pair_pass<1> : k_pair_pass<0>;
         kern<<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, nullptr, nullptr, nullptr, cs, off, n, kb, ke,
                                                        energy, force, part, counter, totals, ctx->d_status);
     }

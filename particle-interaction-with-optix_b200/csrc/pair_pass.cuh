@@ -38,25 +38,13 @@ struct PassAcc {
     unsigned np;
 };
 
-// Non-blocking hint that brings the 128-byte line holding *ptr into L1 (no register is written, so the
-// warp does not wait for it).
-__device__ __forceinline__ void prefetch_l1(const void* ptr) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(ptr));
-}
-
-// Hints for the first lines of window [s, s + L) of float4 records (8 records per line).
-__device__ __forceinline__ void prefetch_window(const float4* __restrict__ p, int s, int L) {
-    if (L > 0) prefetch_l1(p + s);
-    if (L > 8) prefetch_l1(p + s + 8);
-    if (L > 16) prefetch_l1(p + s + 16);
-}
-
 // One pass: window A = [sA, sA + LA), then window B = [offB + LA, offB + L).  OWN: skip j == k.
-// CLAMP: a lane past the end of its windows loads its own record (index k) instead of skipping the
-// load, so no default value has to be kept in registers; the masks discard it either way.
-template <bool PACKED, bool OWN, bool CLAMP = false>
-__device__ __forceinline__ void walk_pass(const float4* __restrict__ p, int k, const float4& pi, int sA, int LA,
-                                          int offB, int L, float rc2, float sig2, PassAcc& a) {
+// Packed form: a lane past the end of its windows loads record kl (a valid index: the target itself,
+// or the last record for a lane without a target) instead of skipping the load, so no default value
+// has to be kept in registers; the masks discard it.
+template <bool PACKED, bool OWN>
+__device__ __forceinline__ void walk_pass(const float4* __restrict__ p, int k, int kl, const float4& pi, int sA,
+                                          int LA, int offB, int L, float rc2, float sig2, PassAcc& a) {
     const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
     if (PACKED) {
         const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
@@ -67,16 +55,8 @@ __device__ __forceinline__ void walk_pass(const float4* __restrict__ p, int k, c
             const bool ok0 = v < L, ok1 = v1 < L;
             const int j0 = v + (v < LA ? sA : offB);
             const int j1 = v1 + (v1 < LA ? sA : offB);
-            float4 q0, q1;
-            if (CLAMP) {
-                q0 = __ldg(&p[ok0 ? j0 : k]);
-                q1 = __ldg(&p[ok1 ? j1 : k]);
-            } else {
-                q0 = pi;
-                q1 = pi;
-                if (ok0) q0 = __ldg(&p[j0]);
-                if (ok1) q1 = __ldg(&p[j1]);
-            }
+            const float4 q0 = __ldg(&p[ok0 ? j0 : kl]);
+            const float4 q1 = __ldg(&p[ok1 ? j1 : kl]);
             bool m0 = ok0, m1 = ok1;
             if (OWN) {
                 m0 = m0 && j0 != k;
@@ -220,63 +200,9 @@ __device__ __forceinline__ void pass_windows(const GridDev& g, const PairParams&
     }
 }
 
-// As pass_windows, in two phases: first every row's cell range [s, e) is read and L1 hints are issued
-// for all of its lines (the ranges of the 32 targets of a warp overlap, so the hints of a warp cover a
-// few dozen distinct lines), then the binary searches run.  The searches and the walk then find the
-// rows in L1 instead of waiting for each first touch in turn.
-__device__ __forceinline__ void pass_windows_pf(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
-                                                const int* __restrict__ off, int obase, int n, const float4& pi, int c,
-                                                int (&ws)[9], int (&wl)[9]) {
-    int cx, cy, cz;
-    decode_cell(g, c, cx, cy, cz);
-    const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
-    const float slack = pp.slack + 8.0f * FLT_EPSILON * fmaxf(fabsf(pi.x), fmaxf(fabsf(pi.y), fabsf(pi.z)));
-    float hs[9];
-#pragma unroll
-    for (int r = 0; r < 9; ++r) {
-        const int dz = r / 3 - 1, dy = r % 3 - 1;
-        const int z = cz + dz, y = cy + dy;
-        hs[r] = -1.f;
-        if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) continue;
-        float dzm = 0.f, dym = 0.f;
-        if (dz < 0) dzm = pi.z - fmaf((float)cz, g.w, g.oz);
-        if (dz > 0) dzm = fmaf((float)(cz + 1), g.w, g.oz) - pi.z;
-        if (dy < 0) dym = pi.y - fmaf((float)cy, g.w, g.oy);
-        if (dy > 0) dym = fmaf((float)(cy + 1), g.w, g.oy) - pi.y;
-        dzm = fmaxf(dzm - slack, 0.f);
-        dym = fmaxf(dym - slack, 0.f);
-        const float d2 = fmaf(dym, dym, dzm * dzm);
-        if (d2 >= pp.rc2w) continue;
-        const int rb = (z * g.gy + y) * g.gx;
-        const int s = min(max(__ldg(&off[rb + xl]) - obase, 0), n);
-        const int e = min(max(__ldg(&off[rb + xh + 1]) - obase, s), n);
-        ws[r] = s;
-        wl[r] = e;
-        hs[r] = sqrtf(pp.rc2w - d2) + slack;
-    }
-#pragma unroll
-    for (int r = 0; r < 9; ++r)
-        if (hs[r] >= 0.f)
-            for (int q = ws[r] & ~7; q < wl[r]; q += 8) prefetch_l1(p + q);
-#pragma unroll
-    for (int r = 0; r < 9; ++r) {
-        if (hs[r] < 0.f) {
-            ws[r] = wl[r] = 0;
-            continue;
-        }
-        const int s = lower_x(p, ws[r], wl[r], pi.x - hs[r]);
-        const int e = upper_x(p, s, wl[r], pi.x + hs[r]);
-        ws[r] = s;
-        wl[r] = e - s;
-    }
-}
-
 // Per-target pass walk.  Every lane of the warp must call it (inactive lanes with active = false):
 // the passes' loop bounds are warp maxima.  MODE 0: scalar, float4 neighbours; 1: packed, float4
-// neighbours; 2: packed, SoA neighbours x2 / y2 / z2 (pairs of the local arrays, even-aligned);
-// 3: as 1 with clamped loads and L1 hints for the next pass's windows issued before each pass;
-// 4: as 1 with the hints only; 5: as 1 with clamped loads only; 6: as 5, with every stencil row's
-// lines hinted into L1 before the window searches (pass_windows_pf).
+// neighbours; 2: packed, SoA neighbours x2 / y2 / z2 (pairs of the local arrays, even-aligned).
 // Indices k, and those of p / x2 / y2 / z2, are local: [0, n).
 template <int MODE>
 __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
@@ -289,10 +215,7 @@ __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& 
     float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (active) {
         pi = __ldg(&p[k]);
-        if (MODE == 6)
-            pass_windows_pf(g, pp, p, off, obase, n, pi, c, ws, wl);
-        else
-            pass_windows(g, pp, p, off, obase, n, pi, c, ws, wl);
+        pass_windows(g, pp, p, off, obase, n, pi, c, ws, wl);
     }
     a.e = a.w = a.fx = a.fy = a.fz = make_float2(0.f, 0.f);
     a.np = 0;
@@ -304,35 +227,197 @@ __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& 
         walk_pass_soa<false>(x2, y2, z2, k, pi, ws[0], ws[0] + wl[0], ws[8], ws[8] + wl[8], rc2, sig2, a);
         walk_pass_soa<false>(x2, y2, z2, k, pi, ws[2], ws[2] + wl[2], ws[6], ws[6] + wl[6], rc2, sig2, a);
     } else {
-        constexpr bool PACKED = MODE != 0;
-        constexpr bool CL = MODE == 3 || MODE == 5 || MODE == 6;
-        constexpr bool PF = MODE == 3 || MODE == 4;
-        if (PF) {
-            prefetch_window(p, ws[3], wl[3]);
-            prefetch_window(p, ws[5], wl[5]);
-        }
-        walk_pass<PACKED, true, CL>(p, k, pi, ws[4], wl[4], 0, wl[4], rc2, sig2, a);
-        if (PF) {
-            prefetch_window(p, ws[1], wl[1]);
-            prefetch_window(p, ws[7], wl[7]);
-        }
-        walk_pass<PACKED, false, CL>(p, k, pi, ws[3], wl[3], ws[5] - wl[3], wl[3] + wl[5], rc2, sig2, a);
-        if (PF) {
-            prefetch_window(p, ws[0], wl[0]);
-            prefetch_window(p, ws[8], wl[8]);
-        }
-        walk_pass<PACKED, false, CL>(p, k, pi, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
-        if (PF) {
-            prefetch_window(p, ws[2], wl[2]);
-            prefetch_window(p, ws[6], wl[6]);
-        }
-        walk_pass<PACKED, false, CL>(p, k, pi, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
-        walk_pass<PACKED, false, CL>(p, k, pi, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
+        constexpr bool PACKED = MODE == 1;
+        const int kl = min(k, n - 1);
+        walk_pass<PACKED, true>(p, k, kl, pi, ws[4], wl[4], 0, wl[4], rc2, sig2, a);
+        walk_pass<PACKED, false>(p, k, kl, pi, ws[3], wl[3], ws[5] - wl[3], wl[3] + wl[5], rc2, sig2, a);
+        walk_pass<PACKED, false>(p, k, kl, pi, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
+        walk_pass<PACKED, false>(p, k, kl, pi, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
+        walk_pass<PACKED, false>(p, k, kl, pi, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
     }
 }
 
 // Copies x, y, z of n sorted float4 records into three arrays (leading dimension ld >= n + 2, two
 // zero pads after the last record so the last even-aligned pair is readable).
 __global__ void k_split_soa(const float4* __restrict__ p, int n, int ld, float* __restrict__ s);
+
+}  // namespace ljc
+
+namespace ljc {
+
+// ---------------------------------------------------------------- two targets per lane
+// Lane l of a warp takes the consecutive sorted targets a = 2m and b = 2m + 1.  When both lie in the
+// same (y, z) row of cells their 9 row windows are merged (per row: one search for the lowest start,
+// one for the highest end, over the row's cells from a's cx - 1 to b's cx + 1), and every candidate
+// loaded once is tested against both targets in one paired FP32 evaluation: the x, y and z
+// differences of (j, a) and (j, b) form the two halves of each packed operand.  Each half rounds as
+// the scalar kernels do, so the distance test and the pair count are those of the single-target
+// walks.  A lane whose targets lie in different rows walks a's windows with b masked; b's own windows
+// are walked afterwards in a second round of passes that only warps holding such a lane take.
+
+struct Pass2Acc {
+    float2 e, w, fx, fy, fz;  // .x target a, .y target b
+    unsigned np;
+};
+
+// One packed evaluation of candidate q (index j) against targets (a, b), minus coordinates in nx/ny/nz.
+template <bool OWN>
+__device__ __forceinline__ void eval2(const float4& q, int j, bool ok, bool useA, bool useB, int ka, int kb,
+                                      float2 nx, float2 ny, float2 nz, float rc2, float2 nsig2, Pass2Acc& a) {
+    bool ma = ok && useA, mb = ok && useB;
+    if (OWN) {
+        ma = ma && j != ka;
+        mb = mb && j != kb;
+    }
+    const float2 dx = __fadd2_rn(make_float2(q.x, q.x), nx);
+    const float2 dy = __fadd2_rn(make_float2(q.y, q.y), ny);
+    const float2 dz = __fadd2_rn(make_float2(q.z, q.z), nz);
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const bool ia = ma && r2.x < rc2, ib = mb && r2.y < rc2;
+    const float2 ir2 = make_float2(ia ? rcp_approx(r2.x) : 0.f, ib ? rcp_approx(r2.y) : 0.f);
+    const float2 s2n = __fmul2_rn(nsig2, ir2);
+    const float2 s4 = __fmul2_rn(s2n, s2n);
+    const float2 ns6 = __fmul2_rn(s4, s2n);
+    const float2 s12 = __fmul2_rn(ns6, ns6);
+    a.e = __fadd2_rn(a.e, __fadd2_rn(s12, ns6));
+    const float2 t = __ffma2_rn(make_float2(2.0f, 2.0f), s12, ns6);
+    a.w = __fadd2_rn(a.w, t);
+    const float2 fsn = __fmul2_rn(t, s2n);
+    a.fx = __ffma2_rn(fsn, dx, a.fx);
+    a.fy = __ffma2_rn(fsn, dy, a.fy);
+    a.fz = __ffma2_rn(fsn, dz, a.fz);
+    a.np += (unsigned)ia + (unsigned)ib;
+}
+
+// One pass of two windows (A = [sA, sA + LA), then B = [offB + LA, offB + L)), two candidates per step.
+// kl: index loaded by a lane past the end of its windows (valid, masked).
+template <bool OWN>
+__device__ __forceinline__ void walk_pass2(const float4* __restrict__ p, int ka, int kb, int kl, bool useA, bool useB,
+                                           float2 nx, float2 ny, float2 nz, int sA, int LA, int offB, int L,
+                                           float rc2, float sig2, Pass2Acc& a) {
+    const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
+    const float2 nsig2 = make_float2(-sig2, -sig2);
+    for (int v = 0; v < maxL; v += 2) {
+        const int v1 = v + 1;
+        const bool ok0 = v < L, ok1 = v1 < L;
+        const int j0 = v + (v < LA ? sA : offB);
+        const int j1 = v1 + (v1 < LA ? sA : offB);
+        const float4 q0 = __ldg(&p[ok0 ? j0 : kl]);
+        const float4 q1 = __ldg(&p[ok1 ? j1 : kl]);
+        eval2<OWN>(q0, j0, ok0, useA, useB, ka, kb, nx, ny, nz, rc2, nsig2, a);
+        eval2<OWN>(q1, j1, ok1, useA, useB, ka, kb, nx, ny, nz, rc2, nsig2, a);
+    }
+}
+
+// Lower bound of the (y, z) distance from position q to stencil row (dy, dz) of cell (cy, cz), minus
+// the slack; d2 >= rc2w culls the row (as pass_windows).
+__device__ __forceinline__ float row_d2(const GridDev& g, int cy, int cz, int dy, int dz, float qy, float qz,
+                                        float slack) {
+    float dzm = 0.f, dym = 0.f;
+    if (dz < 0) dzm = qz - fmaf((float)cz, g.w, g.oz);
+    if (dz > 0) dzm = fmaf((float)(cz + 1), g.w, g.oz) - qz;
+    if (dy < 0) dym = qy - fmaf((float)cy, g.w, g.oy);
+    if (dy > 0) dym = fmaf((float)(cy + 1), g.w, g.oy) - qy;
+    dzm = fmaxf(dzm - slack, 0.f);
+    dym = fmaxf(dym - slack, 0.f);
+    return fmaf(dym, dym, dzm * dzm);
+}
+
+// Merged windows of targets a (cell (cxa, cy, cz)) and, when useB, b (cell (cxb, cy, cz), cxb >= cxa):
+// per row the candidates of both targets' windows (a superset of each), empty when the row is culled
+// for both.  Without useB, a's own windows.
+__device__ __forceinline__ void pass_windows2(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
+                                              const int* __restrict__ off, int obase, int n, const float4& pa,
+                                              const float4& pb, bool useB, int cxa, int cxb, int cy, int cz,
+                                              int (&ws)[9], int (&wl)[9]) {
+    const int xl = max(cxa - 1, 0), xh = min((useB ? cxb : cxa) + 1, g.gx - 1);
+    float m = fmaxf(fabsf(pa.x), fmaxf(fabsf(pa.y), fabsf(pa.z)));
+    if (useB) m = fmaxf(m, fmaxf(fabsf(pb.x), fmaxf(fabsf(pb.y), fabsf(pb.z))));
+    const float slack = pp.slack + 8.0f * FLT_EPSILON * m;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        const int dz = r / 3 - 1, dy = r % 3 - 1;
+        const int z = cz + dz, y = cy + dy;
+        ws[r] = wl[r] = 0;
+        if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) continue;
+        const float d2a = row_d2(g, cy, cz, dy, dz, pa.y, pa.z, slack);
+        const float d2b = useB ? row_d2(g, cy, cz, dy, dz, pb.y, pb.z, slack) : pp.rc2w;
+        const bool la = d2a < pp.rc2w, lb = d2b < pp.rc2w;
+        if (!la && !lb) continue;
+        float lo = 3.4e38f, hi = -3.4e38f;
+        if (la) {
+            const float h = sqrtf(pp.rc2w - d2a) + slack;
+            lo = pa.x - h;
+            hi = pa.x + h;
+        }
+        if (lb) {
+            const float h = sqrtf(pp.rc2w - d2b) + slack;
+            lo = fminf(lo, pb.x - h);
+            hi = fmaxf(hi, pb.x + h);
+        }
+        const int rb = (z * g.gy + y) * g.gx;
+        int s = min(max(__ldg(&off[rb + xl]) - obase, 0), n);
+        int e = min(max(__ldg(&off[rb + xh + 1]) - obase, s), n);
+        s = lower_x(p, s, e, lo);
+        e = upper_x(p, s, e, hi);
+        ws[r] = s;
+        wl[r] = e - s;
+    }
+}
+
+__device__ __forceinline__ void passes2(const float4* __restrict__ p, int ka, int kb, int kl, bool useA, bool useB,
+                                        float2 nx, float2 ny, float2 nz, const int (&ws)[9], const int (&wl)[9],
+                                        float rc2, float sig2, Pass2Acc& a) {
+    walk_pass2<true>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[4], wl[4], 0, wl[4], rc2, sig2, a);
+    walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[3], wl[3], ws[5] - wl[3], wl[3] + wl[5], rc2, sig2, a);
+    walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
+    walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
+    walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
+}
+
+// Both targets of a lane (a = ka, b = ka + 1; activeA / activeB: inside the target range).  Every
+// lane of the warp must call it.  Cells ca, cb are the targets' cells (as read from the sorted cell
+// ids).  Results: a.x for target a, a.y for target b.
+__device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
+                                             const int* __restrict__ off, int obase, int n, int ka, int ca, int cb,
+                                             bool activeA, bool activeB, Pass2Acc& a) {
+    const int kb = ka + 1;
+    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
+    int ws[9], wl[9];
+    int cxa = 0, cya = 0, cza = 0, cxb = 0, cyb = 0, czb = 0;
+    if (activeA) {
+        pa = __ldg(&p[ka]);
+        decode_cell(g, ca, cxa, cya, cza);
+    }
+    if (activeB) {
+        pb = __ldg(&p[kb]);
+        decode_cell(g, cb, cxb, cyb, czb);
+    }
+    const bool same = activeA && activeB && cya == cyb && cza == czb && cxb >= cxa;
+    const bool straddle = activeB && !same;  // b walked in the second round
+    if (activeA) {
+        pass_windows2(g, pp, p, off, obase, n, pa, pb, same, cxa, cxb, cya, cza, ws, wl);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 9; ++r) ws[r] = wl[r] = 0;
+    }
+    a.e = a.w = a.fx = a.fy = a.fz = make_float2(0.f, 0.f);
+    a.np = 0;
+    const float rc2 = pp.rc2, sig2 = pp.sig2;
+    {
+        const float2 nx = make_float2(-pa.x, -pb.x), ny = make_float2(-pa.y, -pb.y), nz = make_float2(-pa.z, -pb.z);
+        passes2(p, ka, kb, min(ka, n - 1), activeA, same, nx, ny, nz, ws, wl, rc2, sig2, a);
+    }
+    if (__any_sync(0xffffffffu, straddle)) {
+        if (straddle) {
+            pass_windows2(g, pp, p, off, obase, n, pb, pb, false, cxb, cxb, cyb, czb, ws, wl);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 9; ++r) ws[r] = wl[r] = 0;
+        }
+        const float2 nx = make_float2(-pb.x, -pb.x), ny = make_float2(-pb.y, -pb.y), nz = make_float2(-pb.z, -pb.z);
+        passes2(p, kb, kb, min(kb, n - 1), false, straddle, nx, ny, nz, ws, wl, rc2, sig2, a);
+    }
+}
 
 }  // namespace ljc

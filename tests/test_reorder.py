@@ -78,7 +78,7 @@ def test_gpu_reorder_out_of_domain_is_reported(torch_cuda, ctx):
 
     torch = torch_cuda
     p = _points(1000)
-    p[10, 0] = 5.0   # key beyond the [0, 1] domain's table
+    p[10, :3] = 50.0   # key 555,500, beyond the 1,111 keys of the [0, 1] domain at radius 0.1
     d = torch.from_numpy(p).cuda()
     with pytest.raises(ljcell.LJError):
         ctx.reorder(d, 0.1)
