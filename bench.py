@@ -43,7 +43,8 @@ METRIC = "LJ pairs/sec @10M particles, plain vs mixed-precision/batched at ≤1e
 FLOP_CANDIDATE = 8
 FLOP_INTERACTING = 18
 KERNEL_NAMES = {1: "k_pair_config", 2: "k_pair_direct<false>", 3: "k_pair_direct<true>", 5: "k_pair_pass<0>",
-                6: "k_pair_pass<1>", 7: "k_pair_pass<2>", 8: "k_pair_pass2<1>", 9: "k_pair_pass2<8>"}
+                6: "k_pair_pass<1>", 7: "k_pair_pass<2>", 8: "k_pair_pass2<1, false>",
+                9: "k_pair_pass2<8, false>", 10: "k_pair_pass2<8, true>"}
 # launches of the pair stage per lj_compute call (kernel 7 first copies x, y, z to SoA arrays)
 PAIR_LAUNCHES = {7: 2}
 

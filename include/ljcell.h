@@ -220,7 +220,7 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  * whose launch shape is fixed at 128 threads per particle, cudaLJ.cu:519-520).
  * Results do not depend on them except in the last bits of floating-point
  * sums.  pair_kernel, for particles binned with LJ_ORDER_X:
- *   0 = default: 9 when the grid averages 2 or more particles per cell, else 6,
+ *   0 = default: 10 when the grid averages 2 or more particles per cell, else 6,
  *   1 = direct: one thread per target, neighbours through L1, its windows
  *       in shared memory,
  *   2 = direct with the windows in registers,
@@ -236,9 +236,10 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  *   8 = row passes with two consecutive targets per lane: their windows
  *       merged, each candidate loaded once and tested against both targets
  *       in one paired FP32 evaluation,
- *   9 = as 8 with the registers capped at 64 per thread (higher occupancy).
+ *   9 = as 8 with the registers capped at 64 per thread (higher occupancy),
+ *  10 = as 9 with the windows parked in shared memory during the walk.
  * With a non-finite coordinate (reported as LJ_ERANGE) the outputs of the
- * particles whose windows hold it are unspecified under 5-9. */
+ * particles whose windows hold it are unspecified under 5-10. */
 typedef struct {
     int pair_kernel;
     int reserved[7];

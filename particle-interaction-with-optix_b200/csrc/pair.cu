@@ -33,12 +33,12 @@ bool dense_grid(int n, const lj_grid& g) {
 }
 
 // Default pair kernel for LJ_ORDER_X (measured on B200, 10M particles): the packed row passes with two
-// targets per lane (kernel 9) from 2 particles per cell up (10 per cell: 2.42 ms against 2.88 ms for one
-// target per lane; 80 per cell: 12.0 ms against 12.6 ms for the SoA walk); below, one target per lane
-// (0.5 per cell: 0.45 ms against 0.48 ms), where the merged windows of two targets add more candidates
-// than the shared loads save.
+// targets per lane (kernel 10) from 2 particles per cell up (10 per cell: 2.38 ms against 2.88 ms for
+// one target per lane; 80 per cell: 11.9 ms against 12.6 ms for the SoA walk); below, one target per
+// lane (0.5 per cell: 0.45 ms against 0.48 ms), where the merged windows of two targets add more
+// candidates than the shared loads save.
 int default_pair_kernel(int n, const lj_grid& g) {
-    return (double)n / ((double)g.dim[0] * g.dim[1] * g.dim[2]) >= kPairCell ? 9 : 6;
+    return (double)n / ((double)g.dim[0] * g.dim[1] * g.dim[2]) >= kPairCell ? 10 : 6;
 }
 
 template <bool XWIN>
@@ -141,6 +141,7 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
             case 7: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 2, energy, force, totals, kb, ke);
             case 8: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 3, energy, force, totals, kb, ke);
             case 9: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 4, energy, force, totals, kb, ke);
+            case 10: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 5, energy, force, totals, kb, ke);
             case 6: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 1, energy, force, totals, kb, ke);
             case 5: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 0, energy, force, totals, kb, ke);
             case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);
@@ -205,8 +206,8 @@ extern "C" lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj
     int best = 1;
     float bt = 3.4e38f;
     lj_status st = LJ_OK;
-    static const int kCandidates[] = {1, 2, 3, 5, 6, 7, 8, 9};
-    for (int ki = 0; ki < 8 && st == LJ_OK; ++ki) {
+    static const int kCandidates[] = {1, 2, 3, 5, 6, 7, 8, 9, 10};
+    for (int ki = 0; ki < 9 && st == LJ_OK; ++ki) {
         const int k = kCandidates[ki];
         ctx->tuning.pair_kernel = k;
         float ms = 3.4e38f;

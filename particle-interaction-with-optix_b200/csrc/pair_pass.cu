@@ -46,13 +46,14 @@ __global__ void __launch_bounds__(kPassThreads) k_pair_pass(GridDev g, PairParam
 }
 
 // Two targets per thread (pass_target2): thread t of the launch takes targets kb + 2t and kb + 2t + 1.
-template <int MINB>
-__global__ void __launch_bounds__(kPassThreads, MINB) k_pair_pass2(GridDev g, PairParams pp, const float4* __restrict__ p,
+// MINB: blocks per SM the register allocation must allow; SMEM: windows parked in shared memory.
+template <int MINB, bool SMEM, int BLOCK = kPassThreads>
+__global__ void __launch_bounds__(BLOCK, MINB) k_pair_pass2(GridDev g, PairParams pp, const float4* __restrict__ p,
                                                              const int* __restrict__ cs, const int* __restrict__ off,
                                                              int n, int kb, int ke, float* __restrict__ energy,
                                                              float* __restrict__ force, Partial* part,
                                                              unsigned* counter, lj_totals* totals, unsigned* status) {
-    const int ka = kb + 2 * (blockIdx.x * kPassThreads + threadIdx.x);
+    const int ka = kb + 2 * (blockIdx.x * BLOCK + threadIdx.x);
     const bool activeA = ka < ke, activeB = ka + 1 < ke;
     const int ncell = g.gx * g.gy * g.gz;
     int ca = 0, cb = 0;
@@ -71,7 +72,12 @@ __global__ void __launch_bounds__(kPassThreads, MINB) k_pair_pass2(GridDev g, Pa
         }
     }
     Pass2Acc a;
-    pass_target2(g, pp, p, off, 0, n, ka, ca, cb, activeA, activeB, a);
+    if (SMEM) {
+        __shared__ int2 s_win[9][BLOCK];
+        pass_target2<BLOCK>(g, pp, p, off, 0, n, ka, ca, cb, activeA, activeB, a, s_win);
+    } else {
+        pass_target2<BLOCK>(g, pp, p, off, 0, n, ka, ca, cb, activeA, activeB, a);
+    }
     const float nf = -pp.fscale;
     if (activeA) {
         if (energy) energy[ka] = pp.e4 * a.e.x;
@@ -89,9 +95,9 @@ __global__ void __launch_bounds__(kPassThreads, MINB) k_pair_pass2(GridDev g, Pa
             force[3 * (size_t)ka + 5] = nf * a.fz.y;
         }
     }
-    reduce_totals<kPassThreads>(0.5 * (double)pp.e4 * ((double)a.e.x + (double)a.e.y),
-                                0.5 * (double)pp.e24 * ((double)a.w.x + (double)a.w.y), (unsigned long long)a.np, part,
-                                counter, totals);
+    reduce_totals<BLOCK>(0.5 * (double)pp.e4 * ((double)a.e.x + (double)a.e.y),
+                         0.5 * (double)pp.e24 * ((double)a.w.x + (double)a.w.y), (unsigned long long)a.np, part,
+                         counter, totals);
 }
 
 __global__ void __launch_bounds__(256) k_split_soa(const float4* __restrict__ p, int n, int ld, float* __restrict__ s) {
@@ -118,12 +124,10 @@ lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, 
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
     const float4* p4 = reinterpret_cast<const float4*>(xyzi);
     const GridDev gd = to_dev(*g);
-    if (mode == 3) {
-        k_pair_pass2<1><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force,
-                                                                  part, counter, totals, ctx->d_status);
-    } else if (mode == 4) {
-        k_pair_pass2<8><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force,
-                                                                  part, counter, totals, ctx->d_status);
+    if (mode >= 3) {
+        auto kern = mode == 3 ? k_pair_pass2<1, false> : (mode == 4 ? k_pair_pass2<8, false> : k_pair_pass2<8, true>);
+        kern<<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force, part, counter,
+                                                       totals, ctx->d_status);
     } else if (mode == 2) {
         const int ld = (n + 2 + 63) & ~63;
         lj_status s = grow(&ctx->soa, &ctx->soa_bytes, 3 * (size_t)ld * sizeof(float));

@@ -375,12 +375,34 @@ __device__ __forceinline__ void passes2(const float4* __restrict__ p, int ka, in
     walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
 }
 
+// As passes2 with the windows read from shared memory (sw[r][threadIdx.x] = (start, length) of row r)
+// at the start of each pass, so they hold no registers during the walk.
+template <int BLOCK>
+__device__ __forceinline__ void passes2_smem(const float4* __restrict__ p, int ka, int kb, int kl, bool useA,
+                                             bool useB, float2 nx, float2 ny, float2 nz, const int2 (*sw)[BLOCK],
+                                             float rc2, float sig2, Pass2Acc& a) {
+    const int t = threadIdx.x;
+    {
+        const int2 w = sw[4][t];
+        walk_pass2<true>(p, ka, kb, kl, useA, useB, nx, ny, nz, w.x, w.y, 0, w.y, rc2, sig2, a);
+    }
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+        // passes (3, 5), (1, 7), (0, 8), (2, 6)
+        const int ra = q == 0 ? 3 : (q == 1 ? 1 : (q == 2 ? 0 : 2));
+        const int2 A = sw[ra][t], B = sw[8 - ra][t];
+        walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, A.x, A.y, B.x - A.y, A.y + B.y, rc2, sig2, a);
+    }
+}
+
 // Both targets of a lane (a = ka, b = ka + 1; activeA / activeB: inside the target range).  Every
 // lane of the warp must call it.  Cells ca, cb are the targets' cells (as read from the sorted cell
 // ids).  Results: a.x for target a, a.y for target b.
+// With sw (shared memory, BLOCK entries per row) the windows are parked there during the walk.
+template <int BLOCK = 128>
 __device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
                                              const int* __restrict__ off, int obase, int n, int ka, int ca, int cb,
-                                             bool activeA, bool activeB, Pass2Acc& a) {
+                                             bool activeA, bool activeB, Pass2Acc& a, int2 (*sw)[BLOCK] = nullptr) {
     const int kb = ka + 1;
     float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
     int ws[9], wl[9];
@@ -406,7 +428,13 @@ __device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams&
     const float rc2 = pp.rc2, sig2 = pp.sig2;
     {
         const float2 nx = make_float2(-pa.x, -pb.x), ny = make_float2(-pa.y, -pb.y), nz = make_float2(-pa.z, -pb.z);
-        passes2(p, ka, kb, min(ka, n - 1), activeA, same, nx, ny, nz, ws, wl, rc2, sig2, a);
+        if (sw) {
+#pragma unroll
+            for (int r = 0; r < 9; ++r) sw[r][threadIdx.x] = make_int2(ws[r], wl[r]);
+            passes2_smem<BLOCK>(p, ka, kb, min(ka, n - 1), activeA, same, nx, ny, nz, sw, rc2, sig2, a);
+        } else {
+            passes2(p, ka, kb, min(ka, n - 1), activeA, same, nx, ny, nz, ws, wl, rc2, sig2, a);
+        }
     }
     if (__any_sync(0xffffffffu, straddle)) {
         if (straddle) {
@@ -416,7 +444,13 @@ __device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams&
             for (int r = 0; r < 9; ++r) ws[r] = wl[r] = 0;
         }
         const float2 nx = make_float2(-pb.x, -pb.x), ny = make_float2(-pb.y, -pb.y), nz = make_float2(-pb.z, -pb.z);
-        passes2(p, kb, kb, min(kb, n - 1), false, straddle, nx, ny, nz, ws, wl, rc2, sig2, a);
+        if (sw) {
+#pragma unroll
+            for (int r = 0; r < 9; ++r) sw[r][threadIdx.x] = make_int2(ws[r], wl[r]);
+            passes2_smem<BLOCK>(p, kb, kb, min(kb, n - 1), false, straddle, nx, ny, nz, sw, rc2, sig2, a);
+        } else {
+            passes2(p, kb, kb, min(kb, n - 1), false, straddle, nx, ny, nz, ws, wl, rc2, sig2, a);
+        }
     }
 }
 
