@@ -101,6 +101,58 @@ __global__ void __launch_bounds__(BLOCK) k_pair_batched(const SysDev* __restrict
         const float2* x2 = reinterpret_cast<const float2*>(soa + S.soa_base);
         const float2* y2 = reinterpret_cast<const float2*>(soa + soa_ld + S.soa_base);
         const float2* z2 = reinterpret_cast<const float2*>(soa + 2 * (size_t)soa_ld + S.soa_base);
+        if (MODE == 3) {
+            // two targets per thread (pass_target2): a = k, b = k + 1, windows parked in shared memory
+            __shared__ int2 s_win[9][BLOCK];
+#pragma unroll
+            for (int r = 0; r < PPT; ++r) {
+                const int k = d.y + 2 * (r * BLOCK + threadIdx.x);
+                const bool activeA = k < d.z, activeB = k + 1 < d.z;
+                int ca = 0, cb = 0;
+                if (activeA) {
+                    ca = __ldg(&cs[k]) - S.cell_base;
+                    if (ca < 0 || ca >= ncell) {
+                        atomicOr(status, kFlagRange);
+                        ca = 0;
+                    }
+                }
+                if (activeB) {
+                    cb = __ldg(&cs[k + 1]) - S.cell_base;
+                    if (cb < 0 || cb >= ncell) {
+                        atomicOr(status, kFlagRange);
+                        cb = 0;
+                    }
+                }
+                Pass2Acc a;
+                pass_target2<BLOCK>(S.g, S.pp, ps, off + S.cell_base, S.first, S.n, k - S.first, ca, cb, activeA,
+                                    activeB, a, s_win);
+                const float nf = -S.pp.fscale;
+                if (activeA) {
+                    if (energy) energy[k] = S.pp.e4 * a.e.x;
+                    if (force) {
+                        force[3 * (size_t)k + 0] = nf * a.fx.x;
+                        force[3 * (size_t)k + 1] = nf * a.fy.x;
+                        force[3 * (size_t)k + 2] = nf * a.fz.x;
+                    }
+                    te[k] = a.e.x;
+                    tw[k] = a.w.x;
+                    tnp[k] = a.np;  // both targets' pairs: the per-system totals only need their sum
+                }
+                if (activeB) {
+                    if (energy) energy[k + 1] = S.pp.e4 * a.e.y;
+                    if (force) {
+                        force[3 * (size_t)k + 3] = nf * a.fx.y;
+                        force[3 * (size_t)k + 4] = nf * a.fy.y;
+                        force[3 * (size_t)k + 5] = nf * a.fz.y;
+                    }
+                    te[k + 1] = a.e.y;
+                    tw[k + 1] = a.w.y;
+                    tnp[k + 1] = 0u;
+                }
+            }
+            __syncthreads();  // s_t is reused by the next tile
+            continue;
+        }
 #pragma unroll
         for (int r = 0; r < PPT; ++r) {
             const int k = d.y + r * BLOCK + threadIdx.x;
@@ -217,7 +269,8 @@ struct lj_batch {
     int* d_firsts = nullptr;
     int4* d_tiles = nullptr;
     int ntiles = 0;
-    int ntiles1 = 0;  // tiles [0, ntiles1) use walk mode 1, the rest mode 2
+    int ntiles1 = 0;  // tiles [0, ntiles1) use walk mode 1, [ntiles1, ntiles2) mode 2, the rest mode 3
+    int ntiles2 = 0;
     size_t tiles_cap = 0;
     unsigned* d_counter = nullptr;
     int* counts = nullptr;
@@ -232,7 +285,7 @@ struct lj_batch {
     int soa_ld = 0;
     int soa_need = 0;
     bool any_soa = false;
-    int persistent_blocks[2] = {0, 0};  // grid of the persistent pair kernel per walk mode
+    int persistent_blocks[3] = {0, 0, 0};  // grid of the persistent pair kernel per walk mode
     // graph replay
     cudaStream_t gstream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -301,7 +354,7 @@ static lj_status build_grids(lj_batch* b) {
         d.cell_base = (int)base;
         d.first = y.first;
         d.n = y.n;
-        d.walk = dense_grid(y.n, g) ? 2 : 1;
+        d.walk = default_pair_kernel(y.n, g) == 10 ? 3 : 1;
         d.soa_base = (int)soa;
         soa += ((long long)y.n + 2 + 1) & ~1LL;
         if (d.walk == 2) b->any_soa = true;
@@ -325,8 +378,9 @@ static std::vector<int4> build_tiles(const lj_batch* b) {
         for (int d = 0; d < 3; ++d) vol *= (double)y.hi[d] - (double)y.lo[d];
         const double rc = y.params.cutoff;
         const double per_target = (double)y.n / (vol > 0 ? vol : 1.0) * rc * rc * rc;
-        for (int k0 = 0; k0 < y.n; k0 += T) {
-            const int k1 = std::min(y.n, k0 + T);
+        const int Ts = b->sd[s].walk == 3 ? 2 * T : T;  // the two-target walk takes 2 targets per thread
+        for (int k0 = 0; k0 < y.n; k0 += Ts) {
+            const int k1 = std::min(y.n, k0 + Ts);
             v.push_back({per_target * (k1 - k0), make_int4(s, y.first + k0, y.first + k1, 0)});
         }
     }
@@ -340,9 +394,9 @@ static std::vector<int4> build_tiles(const lj_batch* b) {
     return out;
 }
 
-static int count_mode1_tiles(const lj_batch* b, const std::vector<int4>& tiles) {
+static int count_tiles_below(const lj_batch* b, const std::vector<int4>& tiles, int walk) {
     int m = 0;
-    while (m < (int)tiles.size() && b->sd[tiles[m].x].walk == 1) ++m;
+    while (m < (int)tiles.size() && b->sd[tiles[m].x].walk < walk) ++m;
     return m;
 }
 
@@ -405,9 +459,10 @@ static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
                                       cudaMemcpyHostToDevice) != cudaSuccess))
         return LJ_ECUDA;
     b->ntiles = (int)tiles.size();
-    b->ntiles1 = count_mode1_tiles(b, tiles);
-    b->persistent_blocks[0] = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread, 1);
-    b->persistent_blocks[1] = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread, 2);
+    b->ntiles1 = count_tiles_below(b, tiles, 2);
+    b->ntiles2 = count_tiles_below(b, tiles, 3);
+    for (int m = 1; m <= 3; ++m)
+        b->persistent_blocks[m - 1] = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread, m);
     ++b->version;
     return LJ_OK;
 }
@@ -436,7 +491,7 @@ static int occ_mode(int threads, int ppt) {
 }
 
 static int batched_occupancy(int threads, int ppt, int mode) {
-    return mode == 2 ? occ_mode<2>(threads, ppt) : occ_mode<1>(threads, ppt);
+    return mode == 3 ? occ_mode<3>(threads, ppt) : (mode == 2 ? occ_mode<2>(threads, ppt) : occ_mode<1>(threads, ppt));
 }
 
 // Tiles [t0, t1) with walk MODE; the persistent grid never exceeds the tile count.
@@ -452,7 +507,8 @@ static void launch_batched_mode(lj_ctx* ctx, lj_batch* b, const float* p4, float
 
 template <int BLOCK, int PPT>
 static void launch_batched_pair(lj_ctx* ctx, lj_batch* b, const float* p4, float* energy, float* force) {
-    launch_batched_mode<BLOCK, PPT, 2>(ctx, b, p4, energy, force, b->ntiles1, b->ntiles);
+    launch_batched_mode<BLOCK, PPT, 3>(ctx, b, p4, energy, force, b->ntiles2, b->ntiles);
+    launch_batched_mode<BLOCK, PPT, 2>(ctx, b, p4, energy, force, b->ntiles1, b->ntiles2);
     launch_batched_mode<BLOCK, PPT, 1>(ctx, b, p4, energy, force, 0, b->ntiles1);
 }
 
@@ -485,7 +541,7 @@ static lj_status batch_step(lj_ctx* ctx, lj_batch* b, const float* x, const floa
                                                         b->soa);
         if ((st = last_launch_status()) != LJ_OK) return st;
     }
-    if (cudaMemsetAsync(b->d_counter, 0, 2 * sizeof(unsigned), s) != cudaSuccess) return LJ_ECUDA;
+    if (cudaMemsetAsync(b->d_counter, 0, 3 * sizeof(unsigned), s) != cudaSuccess) return LJ_ECUDA;
     const int T = b->cfg.threads, P = b->cfg.per_thread;
     if (T == 64)
         P == 1 ? launch_batched_pair<64, 1>(ctx, b, xyzi, energy, force)
@@ -555,8 +611,8 @@ static lj_status batch_graph(lj_ctx* ctx, lj_batch* b, const float* x, const flo
 }
 
 // One plain lj_bin + lj_compute per system (the path the batched step replaces), each with the
-// single-system kernel of the walk the batched kernel takes for it (6: float4 neighbours, 7: SoA pairs),
-// so per-particle results are equal bit for bit.
+// single-system kernel of the walk the batched kernel takes for it (6: float4 neighbours, 7: SoA pairs,
+// 10: two targets per lane), so per-particle results are equal bit for bit.
 static lj_status batch_separate_one(lj_ctx* ctx, lj_batch* b, int s, const float* x, const float* y, const float* z,
                                     float* energy, float* force, int* index, lj_totals* totals);
 
@@ -565,7 +621,7 @@ static lj_status batch_separate(lj_ctx* ctx, lj_batch* b, const float* x, const 
     const lj_tuning saved = ctx->tuning;
     lj_status st = LJ_OK;
     for (int s = 0; s < b->nsys && st == LJ_OK; ++s) {
-        ctx->tuning.pair_kernel = b->sd[s].walk == 2 ? 7 : 6;
+        ctx->tuning.pair_kernel = b->sd[s].walk == 3 ? 10 : (b->sd[s].walk == 2 ? 7 : 6);
         st = batch_separate_one(ctx, b, s, x, y, z, energy, force, index, totals);
     }
     ctx->tuning = saved;
