@@ -316,8 +316,9 @@ LJ_API lj_status lj_batch_autotune(lj_ctx* ctx, lj_batch* b, const float* x, con
  * y, z offsets from the particle's cell origin in cell widths as binary16
  * (stored position = (x, oy + (cy + uy) w, oz + (cz + uz) w)): half the bytes
  * of the float4 layout per neighbour load.  Pair math in FP32 (cell units),
- * each particle's energy and force summed per stencil window and the window
- * sums added with compensation (TwoSum), totals reduced in FP64.  Results
+ * each particle's energy and force summed per stencil window (or per pass of
+ * the row-pass walks) and those sums added with compensation (TwoSum), totals
+ * reduced in FP64.  Results
  * are those of the stored positions: binary16 rounds the y, z offsets to
  * 2^-11 .. 2^-12 of a cell width, and the pair count follows the mixed
  * distance test (d in cell units, r2 < (cutoff / w)^2), restated exactly by
@@ -327,8 +328,9 @@ LJ_API lj_status lj_batch_autotune(lj_ctx* ctx, lj_batch* b, const float* x, con
 LJ_API lj_status lj_pack_mixed(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi,
                                const int* sorted_cell, float* rec);
 /* Energy, force (sorted order) and totals from the records; as lj_compute.
- * The tuning's pair_kernel 2 selects the register-window variant; any other
- * value the shared-memory-window one (the faster of the two on B200). */
+ * Walk by the tuning's pair_kernel: 0 (default) and 8-10 row passes with two
+ * targets per lane; 1 flat walk, windows in shared memory; 2 flat walk,
+ * windows in registers; any other value row passes with one target per lane. */
 LJ_API lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* rec,
                                   const int* sorted_cell, const int* offsets, float* energy, float* force,
                                   lj_totals* totals);

@@ -460,6 +460,230 @@ __global__ void __launch_bounds__(kMixThreads) k_pair_mixed_pass(GridDev g, MixP
                                part, counter, totals);
 }
 
+// ---------------------------------------------------------------- two targets per lane
+// The mixed records on the two-target walk of pair_pass.cuh (pass_target2): lane m takes the
+// consecutive sorted targets a = 2m and b = 2m + 1; when they share a (y, z) row of cells their
+// windows are merged and each record is loaded once and evaluated against both, the two halves of
+// every packed operand holding (j - a) and (j - b) in cell units.  A lane whose targets lie in
+// different rows walks b in a second round.  Each half rounds as k_pair_mixed, so the distance test
+// and the pair count are unchanged; per-target sums are compensated per pass (TwoSum), as above.
+
+struct MixAcc2 {
+    float2 se, ce, sx, cx, sy, cy, sz, cz;  // compensated sums, .x target a, .y target b
+    float2 w;
+    unsigned np;
+};
+
+__device__ __forceinline__ void two_sum_add2(float2& s, float2& c, float2 v) {
+    two_sum_add(s.x, c.x, v.x);
+    two_sum_add(s.y, c.y, v.y);
+}
+
+template <bool OWN>
+__device__ __forceinline__ void mix_walk_pass2(const float2* __restrict__ rec, int ka, int kb, int kl, bool useA,
+                                               bool useB, float2 nx, float2 ntyA, float2 ntzA, float2 ntyB,
+                                               float2 ntzB, int sA, int LA, int offB, int L, const MixParams& mp,
+                                               MixAcc2& a) {
+    const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
+    const float2 invw = f2(mp.invw, mp.invw), nsig2 = f2(-mp.sig2u, -mp.sig2u), two = f2(2.0f, 2.0f);
+    const float rc2 = mp.rc2u;
+    float2 pe = f2(0.f, 0.f), px = pe, py = pe, pz = pe;
+    for (int v = 0; v < maxL; ++v) {
+        const bool ok = v < L;
+        const bool inA = v < LA;
+        const int j = v + (inA ? sA : offB);
+        const float2 q = __ldg(&rec[ok ? j : kl]);
+        bool ma = ok && useA, mb = ok && useB;
+        if (OWN) {
+            ma = ma && j != ka;
+            mb = mb && j != kb;
+        }
+        const float2 u = unpack_yz(q.y);
+        const float2 dx = __fmul2_rn(__fadd2_rn(f2(q.x, q.x), nx), invw);
+        const float2 dy = __fadd2_rn(f2(u.x, u.x), inA ? ntyA : ntyB);
+        const float2 dz = __fadd2_rn(f2(u.y, u.y), inA ? ntzA : ntzB);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const bool ia = ma && r2.x < rc2, ib = mb && r2.y < rc2;
+        const float2 ir2 = f2(ia ? rcp_approx(r2.x) : 0.f, ib ? rcp_approx(r2.y) : 0.f);
+        const float2 s2n = __fmul2_rn(nsig2, ir2);
+        const float2 s4 = __fmul2_rn(s2n, s2n);
+        const float2 ns6 = __fmul2_rn(s4, s2n);
+        const float2 s12 = __fmul2_rn(ns6, ns6);
+        pe = __fadd2_rn(pe, __fadd2_rn(s12, ns6));
+        const float2 t = __ffma2_rn(two, s12, ns6);
+        a.w = __fadd2_rn(a.w, t);
+        const float2 fsn = __fmul2_rn(t, s2n);
+        px = __ffma2_rn(fsn, dx, px);
+        py = __ffma2_rn(fsn, dy, py);
+        pz = __ffma2_rn(fsn, dz, pz);
+        a.np += (unsigned)ia + (unsigned)ib;
+    }
+    two_sum_add2(a.se, a.ce, pe);
+    two_sum_add2(a.sx, a.cx, f2(-px.x, -px.y));
+    two_sum_add2(a.sy, a.cy, f2(-py.x, -py.y));
+    two_sum_add2(a.sz, a.cz, f2(-pz.x, -pz.y));
+}
+
+// Merged mixed windows of a (and b when useB): per row the union of both targets' x windows over the
+// row's cells from a's cx - 1 to b's cx + 1, culled for a target by its cell-unit (y, z) bound.
+__device__ __forceinline__ void mix_windows2(const GridDev& g, const MixParams& mp, const float2* __restrict__ rec,
+                                             const int* __restrict__ off, int n, float xa, float2 ua, float xb,
+                                             float2 ub, bool useB, int cxa, int cxb, int cy, int cz, int (&ws)[9],
+                                             int (&wl)[9]) {
+    const int xl = max(cxa - 1, 0), xh = min((useB ? cxb : cxa) + 1, g.gx - 1);
+    const float slack = mp.slack + 8.0f * FLT_EPSILON * fmaxf(fabsf(xa), useB ? fabsf(xb) : 0.f);
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        const int dz = r / 3 - 1, dy = r % 3 - 1;
+        const int z = cz + dz, y = cy + dy;
+        ws[r] = wl[r] = 0;
+        if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) continue;
+        auto d2_of = [&](float2 u) {
+            float dzm = dz < 0 ? u.y : (dz > 0 ? 1.0f - u.y : 0.f);
+            float dym = dy < 0 ? u.x : (dy > 0 ? 1.0f - u.x : 0.f);
+            dzm = fmaxf(dzm - 1e-5f, 0.f);
+            dym = fmaxf(dym - 1e-5f, 0.f);
+            return fmaf(dym, dym, dzm * dzm);
+        };
+        const float d2a = d2_of(ua);
+        const float d2b = useB ? d2_of(ub) : mp.rc2uw;
+        const bool la = d2a < mp.rc2uw, lb = d2b < mp.rc2uw;
+        if (!la && !lb) continue;
+        float lo = 3.4e38f, hi = -3.4e38f;
+        if (la) {
+            const float h = sqrtf(mp.rc2uw - d2a) * mp.w + slack;
+            lo = xa - h;
+            hi = xa + h;
+        }
+        if (lb) {
+            const float h = sqrtf(mp.rc2uw - d2b) * mp.w + slack;
+            lo = fminf(lo, xb - h);
+            hi = fmaxf(hi, xb + h);
+        }
+        const int rb = (z * g.gy + y) * g.gx;
+        const int s0 = min(max(__ldg(&off[rb + xl]), 0), n);
+        const int e0 = min(max(__ldg(&off[rb + xh + 1]), s0), n);
+        const int lo_i = lower_rx(rec, s0, e0, lo);
+        const int hi_i = upper_rx(rec, lo_i, e0, hi);
+        ws[r] = lo_i;
+        wl[r] = hi_i - lo_i;
+    }
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void mix_passes2(const float2* __restrict__ rec, int ka, int kb, int kl, bool useA,
+                                            bool useB, float2 nx, float2 uy, float2 uz, const int2 (*sw)[BLOCK],
+                                            const MixParams& mp, MixAcc2& a) {
+    const int t = threadIdx.x;
+    // frame of row r for both halves: minus (u - row offset)
+    auto nty = [&](int r) { return f2((float)(r % 3 - 1) - uy.x, (float)(r % 3 - 1) - uy.y); };
+    auto ntz = [&](int r) { return f2((float)(r / 3 - 1) - uz.x, (float)(r / 3 - 1) - uz.y); };
+    {
+        const int2 w = sw[4][t];
+        mix_walk_pass2<true>(rec, ka, kb, kl, useA, useB, nx, nty(4), ntz(4), nty(4), ntz(4), w.x, w.y, 0, w.y, mp, a);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int ra = q == 0 ? 3 : (q == 1 ? 1 : (q == 2 ? 0 : 2));
+        const int rb = 8 - ra;
+        const int2 A = sw[ra][t], B = sw[rb][t];
+        mix_walk_pass2<false>(rec, ka, kb, kl, useA, useB, nx, nty(ra), ntz(ra), nty(rb), ntz(rb), A.x, A.y,
+                              B.x - A.y, A.y + B.y, mp, a);
+    }
+}
+
+__global__ void __launch_bounds__(kMixThreads, 8) k_pair_mixed_pass2(GridDev g, MixParams mp,
+                                                                     const float2* __restrict__ rec,
+                                                                     const int* __restrict__ cs,
+                                                                     const int* __restrict__ off, int n,
+                                                                     float* __restrict__ energy,
+                                                                     float* __restrict__ force, Partial* part,
+                                                                     unsigned* counter, lj_totals* totals,
+                                                                     unsigned* status) {
+    __shared__ int2 s_win[9][kMixThreads];
+    const int ka = 2 * (blockIdx.x * kMixThreads + threadIdx.x);
+    const int kb = ka + 1;
+    const bool activeA = ka < n, activeB = kb < n;
+    const int ncell = g.gx * g.gy * g.gz;
+    float xa = 0.f, xb = 0.f;
+    float2 ua = f2(0.f, 0.f), ub = ua;
+    int cxa = 0, cya = 0, cza = 0, cxb = 0, cyb = 0, czb = 0;
+    if (activeA) {
+        const float2 r = __ldg(&rec[ka]);
+        xa = r.x;
+        ua = unpack_yz(r.y);
+        int c = __ldg(&cs[ka]);
+        if (c < 0 || c >= ncell) {
+            atomicOr(status, kFlagRange);
+            c = 0;
+        }
+        decode_cell(g, c, cxa, cya, cza);
+    }
+    if (activeB) {
+        const float2 r = __ldg(&rec[kb]);
+        xb = r.x;
+        ub = unpack_yz(r.y);
+        int c = __ldg(&cs[kb]);
+        if (c < 0 || c >= ncell) {
+            atomicOr(status, kFlagRange);
+            c = 0;
+        }
+        decode_cell(g, c, cxb, cyb, czb);
+    }
+    const bool same = activeA && activeB && cya == cyb && cza == czb && cxb >= cxa;
+    const bool straddle = activeB && !same;
+    MixAcc2 a;
+    a.se = a.ce = a.sx = a.cx = a.sy = a.cy = a.sz = a.cz = a.w = f2(0.f, 0.f);
+    a.np = 0;
+    {
+        int ws[9], wl[9];
+        if (activeA) {
+            mix_windows2(g, mp, rec, off, n, xa, ua, xb, ub, same, cxa, cxb, cya, cza, ws, wl);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 9; ++r) ws[r] = wl[r] = 0;
+        }
+#pragma unroll
+        for (int r = 0; r < 9; ++r) s_win[r][threadIdx.x] = make_int2(ws[r], wl[r]);
+    }
+    mix_passes2<kMixThreads>(rec, ka, kb, min(ka, n - 1), activeA, same, f2(-xa, -xb), f2(ua.x, ub.x),
+                             f2(ua.y, ub.y), s_win, mp, a);
+    if (__any_sync(0xffffffffu, straddle)) {
+        {
+            int ws[9], wl[9];
+            if (straddle) {
+                mix_windows2(g, mp, rec, off, n, xb, ub, xb, ub, false, cxb, cxb, cyb, czb, ws, wl);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 9; ++r) ws[r] = wl[r] = 0;
+            }
+#pragma unroll
+            for (int r = 0; r < 9; ++r) s_win[r][threadIdx.x] = make_int2(ws[r], wl[r]);
+        }
+        mix_passes2<kMixThreads>(rec, kb, kb, min(kb, n - 1), false, straddle, f2(-xb, -xb), f2(ub.x, ub.x),
+                                 f2(ub.y, ub.y), s_win, mp, a);
+    }
+    if (activeA) {
+        if (energy) energy[ka] = mp.e4 * (a.se.x + a.ce.x);
+        if (force) {
+            force[3 * (size_t)ka + 0] = mp.fscale * (a.sx.x + a.cx.x);
+            force[3 * (size_t)ka + 1] = mp.fscale * (a.sy.x + a.cy.x);
+            force[3 * (size_t)ka + 2] = mp.fscale * (a.sz.x + a.cz.x);
+        }
+    }
+    if (activeB) {
+        if (energy) energy[kb] = mp.e4 * (a.se.y + a.ce.y);
+        if (force) {
+            force[3 * (size_t)kb + 0] = mp.fscale * (a.sx.y + a.cx.y);
+            force[3 * (size_t)kb + 1] = mp.fscale * (a.sy.y + a.cy.y);
+            force[3 * (size_t)kb + 2] = mp.fscale * (a.sz.y + a.cz.y);
+        }
+    }
+    reduce_totals<kMixThreads>(
+        0.5 * (double)mp.e4 * ((double)a.se.x + (double)a.ce.x + (double)a.se.y + (double)a.ce.y),
+        0.5 * (double)mp.e24 * ((double)a.w.x + (double)a.w.y), (unsigned long long)a.np, part, counter, totals);
+}
+
 }  // namespace ljc
 
 using namespace ljc;
@@ -500,7 +724,9 @@ extern "C" lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_pa
     mp.e24 = 24.0f * p->epsilon;
     mp.fscale = -mp.e24 * g->width / sig2;
     mp.slack = grid_slack(*g);
-    const int blocks = (n + kMixThreads - 1) / kMixThreads;
+    const bool two = ctx->tuning.pair_kernel == 0 || ctx->tuning.pair_kernel >= 8;  // two targets per lane
+    const int per_block = two ? 2 * kMixThreads : kMixThreads;
+    const int blocks = (n + per_block - 1) / per_block;
     const size_t need = 256 + (size_t)blocks * sizeof(Partial);
     if (need > ctx->red_bytes) {
         lj_status s = grow(&ctx->red, &ctx->red_bytes, need);
@@ -509,9 +735,15 @@ extern "C" lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_pa
     }
     unsigned* counter = static_cast<unsigned*>(ctx->red);
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
-    // row passes unless pair_kernel 1 (windows in shared memory) or 2 (windows in registers) asks for a
-    // flat walk
-    if (ctx->tuning.pair_kernel != 1 && ctx->tuning.pair_kernel != 2)
+    // row passes with two targets per lane by default (and with the tuning's two-target kernels 8-10);
+    // pair_kernel 1 (windows in shared memory) or 2 (windows in registers) asks for a flat walk, the
+    // others for row passes with one target per lane
+    if (two)
+        k_pair_mixed_pass2<<<blocks, kMixThreads, 0, ctx->stream>>>(to_dev(*g), mp,
+                                                                    reinterpret_cast<const float2*>(rec), sorted_cell,
+                                                                    offsets, n, energy, force, part, counter, totals,
+                                                                    ctx->d_status);
+    else if (ctx->tuning.pair_kernel != 1 && ctx->tuning.pair_kernel != 2)
         k_pair_mixed_pass<<<blocks, kMixThreads, 0, ctx->stream>>>(to_dev(*g), mp,
                                                                    reinterpret_cast<const float2*>(rec), sorted_cell,
                                                                    offsets, n, energy, force, part, counter, totals,

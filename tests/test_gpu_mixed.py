@@ -18,7 +18,9 @@ FORCE_NORMWISE_TOL = 1e-5
 TOTAL_ENERGY_TOL = 1e-6
 
 
-@pytest.mark.parametrize("kernel", [1, 2])   # windows in shared memory / in registers
+# 0: default (row passes, two targets per lane); 1 / 2: flat walk, windows in shared memory / in
+# registers; 6: row passes, one target per lane
+@pytest.mark.parametrize("kernel", [0, 1, 2, 6])
 @pytest.mark.parametrize("name", ["uniform_c1", "uniform_dense", "shell", "tiny33"])
 def test_mixed_against_oracle(torch_cuda, ctx, name, kernel):
     import ljcell
