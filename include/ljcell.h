@@ -341,6 +341,26 @@ LJ_API lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params
  * lj_sync returns LJ_ETIMEOUT and the context stays usable.  ncells > 4096. */
 LJ_API lj_status lj_test_scan_withheld_tile(lj_ctx* ctx, const int* counts, long long ncells, int* offsets);
 
+/* ------------------------------------------------------------- time step
+ * One velocity-Verlet step of the truncated law with rebinning (no stage of
+ * the reference, whose ParticlesContainer swap and per-particle cuRAND state,
+ * cudaLJ.cu:69-76 and :96-97, anticipate particles moving between steps).
+ * State, all device, in sorted order as lj_bin (LJ_ORDER_X) leaves it:
+ *   xyzi[4n]      records (x, y, z, caller's particle id bits), 16-byte aligned
+ *   vel[3n]       velocities
+ *   force[3n]     forces of the current positions (lj_compute, or the last step)
+ *   sorted_cell[n], counts[ncells], offsets[ncells + 1]  the cell grid of g
+ * The step: v += h F (h = dt / (2 mass)); x += dt v; rebin the moved particles
+ * from the current order; carry v and the ids to the new order; F = forces of
+ * the new positions; v += h F.  Each update is one IEEE multiply and one add
+ * (no fused multiply-add), in single precision.  On return every state array
+ * holds the new sorted state; energy[n] (optional) and totals (optional) are
+ * those of the new positions, as lj_compute writes them.  Scratch: 28 bytes
+ * per particle in the context.  Asynchronous on the context's stream. */
+LJ_API lj_status lj_step_verlet(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, float dt, float mass,
+                                float* xyzi, float* vel, float* force, int* sorted_cell, int* counts, int* offsets,
+                                float* energy, lj_totals* totals);
+
 /* ------------------------------------------------------------- spatial sort
  * Replaces reorder(N, points, radius) (SDK/optixMultiSphereAABB/sort.cu:29-41,
  * key kernel count_per_cell :7-18): sorts n float4 points in place by the key

@@ -404,3 +404,17 @@ def reorder(points: np.ndarray, radius: float) -> np.ndarray:
     out = p[order].copy()
     out[:, 3] = w[order]
     return out
+
+
+# --------------------------------------------------------------------- time step
+def verlet_drift(xyz: np.ndarray, vel: np.ndarray, force: np.ndarray, dt: float, mass: float):
+    """Half kick and drift of lj_step_verlet in single precision, one IEEE
+    multiply and one add per update (numpy float32 arithmetic does not fuse):
+    h = 0.5 * dt / mass; v' = v + h F; x' = x + dt v'.  The reference has no
+    time step (its ParticlesContainer swap and cuRAND state, cudaLJ.cu:69-76
+    and :96-97, anticipate one); this is the restatement the GPU step is
+    checked against.  Returns (x', v', h), arrays (n, 3) float32."""
+    h = np.float32(np.float32(0.5) * np.float32(dt) / np.float32(mass))
+    v2 = (vel.astype(np.float32) + h * force.astype(np.float32)).astype(np.float32)
+    x2 = (xyz.astype(np.float32) + np.float32(dt) * v2).astype(np.float32)
+    return x2, v2, h

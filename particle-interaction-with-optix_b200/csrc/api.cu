@@ -111,6 +111,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->e2e);
     cudaFree(c->soa);
     cudaFree(c->reorder);
+    cudaFree(c->step);
     if (c->e2e_ready) {
         cudaStreamSynchronize(c->copy_stream);
         for (int i = 0; i < 8; ++i) cudaEventDestroy(c->e2e_ev[i]);

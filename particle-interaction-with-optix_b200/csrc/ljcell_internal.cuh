@@ -103,6 +103,8 @@ struct lj_ctx {
     size_t soa_bytes;
     void* reorder;               // lj_reorder: key counts, offsets, sorted records and their keys
     size_t reorder_bytes;
+    void* step;                  // lj_step_verlet: moved positions, half-kicked velocities, ids
+    size_t step_bytes;
     // end-to-end buffers (lj_simulate_host): device buffers, a second stream for the device-to-host
     // copies and the events that order it after the pair chunks
     void* e2e;

@@ -125,6 +125,8 @@ def _load() -> C.CDLL:
         "lj_compute_mixed": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp]),
         "lj_test_scan_withheld_tile": (i32, [vp, vp, i64, vp]),
         "lj_reorder": (i32, [vp, i32, vp, C.c_float]),
+        "lj_step_verlet": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, C.c_float, C.c_float, vp, vp, vp, vp,
+                                 vp, vp, vp, vp]),
         "lj_simulate_host": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
                                    C.POINTER(Totals)]),
     }
@@ -142,7 +144,7 @@ ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj
                "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_autotune_compute", "lj_batch_create",
                "lj_batch_destroy", "lj_batch_get_config", "lj_batch_grid", "lj_batch_run", "lj_batch_run_graph",
                "lj_batch_run_separate", "lj_batch_autotune", "lj_pack_mixed", "lj_compute_mixed",
-               "lj_test_scan_withheld_tile", "lj_reorder", "lj_simulate_host")
+               "lj_test_scan_withheld_tile", "lj_reorder", "lj_step_verlet", "lj_simulate_host")
 
 
 def lib() -> C.CDLL:
@@ -394,6 +396,15 @@ class Context:
         n = int(points.shape[0]) if points.numel() else 0
         _check(_lib.lj_reorder(self._h, n, _ptr(points), C.c_float(radius)), "lj_reorder")
         return points
+
+    def step_verlet(self, g: Grid, p: Params, b: Binned, vel, force, dt: float, mass: float = 1.0, energy=None,
+                    totals=None):
+        """lj_step_verlet: one velocity-Verlet step of the binned system b (LJ_ORDER_X) in place: b.xyzi,
+        b.cell, b.counts, b.offsets, vel (n, 3) and force (n, 3) hold the new sorted state afterwards."""
+        _check(_lib.lj_step_verlet(self._h, C.byref(g), C.byref(p), b.n, C.c_float(dt), C.c_float(mass),
+                                   _ptr(b.xyzi), _ptr(vel), _ptr(force), _ptr(b.cell), _ptr(b.counts),
+                                   _ptr(b.offsets), _ptr(energy), _ptr(totals)), "lj_step_verlet")
+        return b
 
     def simulate_host(self, g: Grid, p: Params, hx: np.ndarray, hy: np.ndarray, hz: np.ndarray,
                       energy: np.ndarray | None = None, force: np.ndarray | None = None,
