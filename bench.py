@@ -510,7 +510,7 @@ def mixed_workload(ctx, cfg, seed, flush, reps=10):
 
     t_pack = time_events(lambda: ctx.pack_mixed(g, b, rec), reps, flush)
     mixed_ms = {}
-    for mk in (0, 1, 2):   # the mixed kernel's walks (row passes, flat with two window layouts); keep the fastest
+    for mk in (0, 1, 2):   # the mixed walks (two-target row passes, flat with two window layouts); keep the fastest
         ctx.set_tuning(mk)
         mixed_ms[mk] = time_events(mixed_step, reps, flush)
     mk = min(mixed_ms, key=mixed_ms.get)
@@ -521,7 +521,7 @@ def mixed_workload(ctx, cfg, seed, flush, reps=10):
     mixed_pairs = ljcell.totals_from_tensor(tot)["pairs"]
     out = {"workload": cfg["workload"] + ", mixed precision", "ms_pair_plain": t_plain,
            "plain_kernel": KERNEL_NAMES[kern], "ms_pack_mixed": t_pack, "ms_pack_and_pair_mixed": t_mixed,
-           "mixed_kernel": {0: "k_pair_mixed_pass", 1: "k_pair_mixed", 2: "k_pair_mixed_reg"}[mk],
+           "mixed_kernel": {0: "k_pair_mixed_pass2", 1: "k_pair_mixed", 2: "k_pair_mixed_reg"}[mk],
            "speedup_vs_plain": t_plain / t_mixed, "pairs_plain": plain_pairs, "pairs_mixed": mixed_pairs,
            "errors": "stated by tests/test_gpu_mixed.py::test_mixed_dense_sample (FP64 oracle on a target sample)"}
     del soa, b, e, f, tot, rec
