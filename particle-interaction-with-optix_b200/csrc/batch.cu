@@ -28,8 +28,8 @@ struct SysDev {
     int cell_base;
     int first;
     int n;
-    int walk;      // pass_target mode: 1 = float4 neighbours, 2 = SoA pairs (the single-system default's choice)
-    int soa_base;  // even start of the system's x / y / z in the SoA copies
+    int walk;  // 1: one target per lane (kernel 6's walk), 3: two targets per lane (kernel 10's), as the
+               // single-system default chooses for the system
 };
 
 // ---------------------------------------------------------------- count
@@ -74,14 +74,15 @@ __global__ void __launch_bounds__(256) k_count_batched(const SysDev* __restrict_
 
 // ---------------------------------------------------------------- pair (persistent, tile queue)
 // Tile = (system, k0, k1): targets [k0, k1) of one system, at most
-// BLOCK * PPT of them.  Each target runs the single-system default's
-// per-target routine (pass_target, in the system's local indices), so
-// per-particle results equal a per-system lj_compute bit for bit.  One launch
-// per walk mode (MODE), over the tiles of the systems using it.  Per-target
-// raw sums go to te / tw / tnp for the per-system totals.
+// BLOCK * PPT of them (2 * BLOCK * PPT for MODE 3).  Each target runs the
+// per-target routine of the single-system kernel the default picks for the
+// system (MODE 1: pass_target, one target per lane, as kernel 6; MODE 3:
+// pass_target2, two targets per lane, as kernel 10), in the system's local
+// indices, so per-particle results equal a per-system lj_compute with that
+// kernel bit for bit.  One launch per walk mode, over the tiles of the systems
+// using it.  Per-target raw sums go to te / tw / tnp for the per-system totals.
 template <int BLOCK, int PPT, int MODE>
 __global__ void __launch_bounds__(BLOCK) k_pair_batched(const SysDev* __restrict__ sys, const float4* __restrict__ p,
-                                                        const float* __restrict__ soa, int soa_ld,
                                                         const int* __restrict__ cs, const int* __restrict__ off,
                                                         const int4* __restrict__ tiles, int ntiles,
                                                         unsigned* tile_counter, float* __restrict__ energy,
@@ -98,9 +99,6 @@ __global__ void __launch_bounds__(BLOCK) k_pair_batched(const SysDev* __restrict
         const SysDev S = sys[d.x];
         const int ncell = S.g.gx * S.g.gy * S.g.gz;
         const float4* ps = p + S.first;
-        const float2* x2 = reinterpret_cast<const float2*>(soa + S.soa_base);
-        const float2* y2 = reinterpret_cast<const float2*>(soa + soa_ld + S.soa_base);
-        const float2* z2 = reinterpret_cast<const float2*>(soa + 2 * (size_t)soa_ld + S.soa_base);
         if (MODE == 3) {
             // two targets per thread (pass_target2): a = k, b = k + 1, windows parked in shared memory
             __shared__ int2 s_win[9][BLOCK];
@@ -166,7 +164,8 @@ __global__ void __launch_bounds__(BLOCK) k_pair_batched(const SysDev* __restrict
                 }
             }
             PassAcc a;
-            pass_target<MODE>(S.g, S.pp, ps, x2, y2, z2, off + S.cell_base, S.first, S.n, k - S.first, c, active, a);
+            pass_target<MODE>(S.g, S.pp, ps, nullptr, nullptr, nullptr, off + S.cell_base, S.first, S.n, k - S.first, c,
+                              active, a);
             if (active) {
                 const float ea = a.e.x + a.e.y;
                 if (energy) energy[k] = S.pp.e4 * ea;
@@ -185,30 +184,6 @@ __global__ void __launch_bounds__(BLOCK) k_pair_batched(const SysDev* __restrict
     }
 }
 
-// SoA copies of the sorted positions of the systems that read neighbours as SoA pairs, each system
-// at its even soa_base (the zero pads between systems are set once when the plan is built).
-__global__ void __launch_bounds__(256) k_split_soa_batched(const SysDev* __restrict__ sys,
-                                                           const int* __restrict__ firsts, int nsys,
-                                                           const float4* __restrict__ p, int n, int ld,
-                                                           float* __restrict__ soa) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int lo = 0, hi = nsys - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(&firsts[mid]) <= i)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        const SysDev& S = sys[lo];
-        if (S.walk != 2) continue;
-        const float4 q = p[i];
-        const int j = S.soa_base + (i - S.first);
-        soa[j] = q.x;
-        soa[ld + j] = q.y;
-        soa[2 * (size_t)ld + j] = q.z;
-    }
-}
 
 // One block per system: totals from the per-target sums, in index order.
 __global__ void __launch_bounds__(256) k_sys_totals(const SysDev* __restrict__ sys, const float* __restrict__ te,
@@ -269,8 +244,7 @@ struct lj_batch {
     int* d_firsts = nullptr;
     int4* d_tiles = nullptr;
     int ntiles = 0;
-    int ntiles1 = 0;  // tiles [0, ntiles1) use walk mode 1, [ntiles1, ntiles2) mode 2, the rest mode 3
-    int ntiles2 = 0;
+    int ntiles1 = 0;  // tiles [0, ntiles1) use walk mode 1, the rest mode 3
     size_t tiles_cap = 0;
     unsigned* d_counter = nullptr;
     int* counts = nullptr;
@@ -281,10 +255,6 @@ struct lj_batch {
     float* te = nullptr;
     float* tw = nullptr;
     unsigned* tnp = nullptr;
-    float* soa = nullptr;  // x, y, z of systems that read SoA pairs, leading dimension soa_ld
-    int soa_ld = 0;
-    int soa_need = 0;
-    bool any_soa = false;
     int persistent_blocks[3] = {0, 0, 0};  // grid of the persistent pair kernel per walk mode
     // graph replay
     cudaStream_t gstream = nullptr;
@@ -309,9 +279,6 @@ static void free_plan_buffers(lj_batch* b) {
     cudaFree(b->te);
     cudaFree(b->tw);
     cudaFree(b->tnp);
-    cudaFree(b->soa);
-    b->soa = nullptr;
-    b->soa_ld = 0;
     b->d_sys = nullptr;
     b->d_binsys = nullptr;
     b->d_firsts = nullptr;
@@ -334,8 +301,7 @@ static bool valid_config(const lj_batch_config& c) {
 static lj_status build_grids(lj_batch* b) {
     b->grids.resize(b->nsys);
     b->sd.resize(b->nsys);
-    b->any_soa = false;
-    long long base = 0, soa = 0;
+    long long base = 0;
     for (int s = 0; s < b->nsys; ++s) {
         const lj_system& y = b->sys[s];
         const float w = y.params.cutoff * b->cfg.cell_multiple;
@@ -355,20 +321,16 @@ static lj_status build_grids(lj_batch* b) {
         d.first = y.first;
         d.n = y.n;
         d.walk = default_pair_kernel(y.n, g) == 10 ? 3 : 1;
-        d.soa_base = (int)soa;
-        soa += ((long long)y.n + 2 + 1) & ~1LL;
-        if (d.walk == 2) b->any_soa = true;
         base += (long long)g.dim[0] * g.dim[1] * g.dim[2];
-        if (base > 2147483646LL || soa > 2147483646LL) return LJ_EUNSUPPORTED;
+        if (base > 2147483646LL) return LJ_EUNSUPPORTED;
     }
     b->total_cells = base;
-    b->soa_need = (int)((soa + 63) & ~63LL);
     return LJ_OK;
 }
 
-// Tiles of T = threads * per_thread consecutive targets per system: first those of the systems
-// walked with mode 1, then mode 2, each group ordered by estimated cost (targets x expected
-// candidates: n / box volume x cutoff^3), largest first.
+// Tiles of T = threads * per_thread consecutive targets per system (2T for systems on the two-target
+// walk): first those of the systems walked with mode 1, then mode 3, each group ordered by estimated
+// cost (targets x expected candidates: n / box volume x cutoff^3), largest first.
 static std::vector<int4> build_tiles(const lj_batch* b) {
     const int T = b->cfg.threads * b->cfg.per_thread;
     std::vector<std::pair<double, int4>> v;
@@ -427,11 +389,6 @@ static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
             (st = dev_alloc(&b->d_counter, (size_t)64)) != LJ_OK)
             return st;
     }
-    if (!b->soa) {
-        if ((st = dev_alloc(&b->soa, 3 * (size_t)b->soa_need)) != LJ_OK) return st;
-        if (cudaMemset(b->soa, 0, 3 * (size_t)b->soa_need * sizeof(float)) != cudaSuccess) return LJ_ECUDA;
-        b->soa_ld = b->soa_need;
-    }
     if ((size_t)b->total_cells + 1 > b->cells_cap) {
         cudaFree(b->counts);
         cudaFree(b->offsets);
@@ -459,10 +416,9 @@ static lj_status build_plan(lj_ctx* ctx, lj_batch* b) {
                                       cudaMemcpyHostToDevice) != cudaSuccess))
         return LJ_ECUDA;
     b->ntiles = (int)tiles.size();
-    b->ntiles1 = count_tiles_below(b, tiles, 2);
-    b->ntiles2 = count_tiles_below(b, tiles, 3);
-    for (int m = 1; m <= 3; ++m)
-        b->persistent_blocks[m - 1] = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread, m);
+    b->ntiles1 = count_tiles_below(b, tiles, 3);
+    b->persistent_blocks[0] = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread, 1);
+    b->persistent_blocks[2] = ctx->sm_count * batched_occupancy(b->cfg.threads, b->cfg.per_thread, 3);
     ++b->version;
     return LJ_OK;
 }
@@ -491,7 +447,7 @@ static int occ_mode(int threads, int ppt) {
 }
 
 static int batched_occupancy(int threads, int ppt, int mode) {
-    return mode == 3 ? occ_mode<3>(threads, ppt) : (mode == 2 ? occ_mode<2>(threads, ppt) : occ_mode<1>(threads, ppt));
+    return mode == 3 ? occ_mode<3>(threads, ppt) : occ_mode<1>(threads, ppt);
 }
 
 // Tiles [t0, t1) with walk MODE; the persistent grid never exceeds the tile count.
@@ -501,14 +457,13 @@ static void launch_batched_mode(lj_ctx* ctx, lj_batch* b, const float* p4, float
     if (t1 <= t0) return;
     const int grid = std::min(b->persistent_blocks[MODE - 1], t1 - t0);
     k_pair_batched<BLOCK, PPT, MODE><<<grid, BLOCK, 0, ctx->stream>>>(
-        b->d_sys, reinterpret_cast<const float4*>(p4), b->soa, b->soa_ld, b->cell, b->offsets, b->d_tiles + t0,
+        b->d_sys, reinterpret_cast<const float4*>(p4), b->cell, b->offsets, b->d_tiles + t0,
         t1 - t0, b->d_counter + (MODE - 1), energy, force, b->te, b->tw, b->tnp, ctx->d_status);
 }
 
 template <int BLOCK, int PPT>
 static void launch_batched_pair(lj_ctx* ctx, lj_batch* b, const float* p4, float* energy, float* force) {
-    launch_batched_mode<BLOCK, PPT, 3>(ctx, b, p4, energy, force, b->ntiles2, b->ntiles);
-    launch_batched_mode<BLOCK, PPT, 2>(ctx, b, p4, energy, force, b->ntiles1, b->ntiles2);
+    launch_batched_mode<BLOCK, PPT, 3>(ctx, b, p4, energy, force, b->ntiles1, b->ntiles);
     launch_batched_mode<BLOCK, PPT, 1>(ctx, b, p4, energy, force, 0, b->ntiles1);
 }
 
@@ -534,13 +489,6 @@ static lj_status batch_step(lj_ctx* ctx, lj_batch* b, const float* x, const floa
                          index ? &sorted : nullptr, xyzi, b->cell, GridDev{}, b->d_binsys, b->d_firsts, b->nsys)) !=
         LJ_OK)
         return st;
-    if (b->any_soa && n > 0) {
-        long long blocks = ((long long)n + 255) / 256;
-        if (blocks > (long long)ctx->sm_count * 8) blocks = (long long)ctx->sm_count * 8;
-        k_split_soa_batched<<<(int)blocks, 256, 0, s>>>(b->d_sys, b->d_firsts, b->nsys, b->xyzi, n, b->soa_ld,
-                                                        b->soa);
-        if ((st = last_launch_status()) != LJ_OK) return st;
-    }
     if (cudaMemsetAsync(b->d_counter, 0, 3 * sizeof(unsigned), s) != cudaSuccess) return LJ_ECUDA;
     const int T = b->cfg.threads, P = b->cfg.per_thread;
     if (T == 64)
@@ -611,8 +559,8 @@ static lj_status batch_graph(lj_ctx* ctx, lj_batch* b, const float* x, const flo
 }
 
 // One plain lj_bin + lj_compute per system (the path the batched step replaces), each with the
-// single-system kernel of the walk the batched kernel takes for it (6: float4 neighbours, 7: SoA pairs,
-// 10: two targets per lane), so per-particle results are equal bit for bit.
+// single-system kernel of the walk the batched kernel takes for it (6: one target per lane, 10: two
+// targets per lane), so per-particle results are equal bit for bit.
 static lj_status batch_separate_one(lj_ctx* ctx, lj_batch* b, int s, const float* x, const float* y, const float* z,
                                     float* energy, float* force, int* index, lj_totals* totals);
 
@@ -621,7 +569,7 @@ static lj_status batch_separate(lj_ctx* ctx, lj_batch* b, const float* x, const 
     const lj_tuning saved = ctx->tuning;
     lj_status st = LJ_OK;
     for (int s = 0; s < b->nsys && st == LJ_OK; ++s) {
-        ctx->tuning.pair_kernel = b->sd[s].walk == 3 ? 10 : (b->sd[s].walk == 2 ? 7 : 6);
+        ctx->tuning.pair_kernel = b->sd[s].walk == 3 ? 10 : 6;
         st = batch_separate_one(ctx, b, s, x, y, z, energy, force, index, totals);
     }
     ctx->tuning = saved;

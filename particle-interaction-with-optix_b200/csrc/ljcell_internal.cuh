@@ -133,8 +133,6 @@ lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const flo
                      int nsys);
 // Default pair kernel (lj_tuning numbering) for n particles binned in g with LJ_ORDER_X (pair.cu).
 int default_pair_kernel(int n, const lj_grid& g);
-// True when g averages enough particles per cell for the walks that read SoA neighbour pairs (pair.cu).
-bool dense_grid(int n, const lj_grid& g);
 // Pair stage of lj_compute over the sorted targets [kb, ke) (pair.cu); totals cover those targets only.
 lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm, int n, const float* xyzi,
                              const int* cs, const int* off, lj_order order, float* energy, float* force,

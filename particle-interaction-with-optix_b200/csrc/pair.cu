@@ -25,12 +25,7 @@
 
 namespace ljc {
 
-constexpr double kDenseCell = 32.0;  // particles per cell from which the batched kernel reads SoA pairs
 constexpr double kPairCell = 2.0;    // particles per cell from which the default takes two targets per lane
-
-bool dense_grid(int n, const lj_grid& g) {
-    return (double)n / ((double)g.dim[0] * g.dim[1] * g.dim[2]) >= kDenseCell;
-}
 
 // Default pair kernel for LJ_ORDER_X (measured on B200, 10M particles): the packed row passes with two
 // targets per lane (kernel 10) from 2 particles per cell up (10 per cell: 2.38 ms against 2.88 ms for
