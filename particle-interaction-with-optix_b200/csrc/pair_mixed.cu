@@ -488,11 +488,7 @@ __device__ __forceinline__ void mix_walk_pass2(const float2* __restrict__ rec, i
     const float2 invw = f2(mp.invw, mp.invw), nsig2 = f2(-mp.sig2u, -mp.sig2u), two = f2(2.0f, 2.0f);
     const float rc2 = mp.rc2u;
     float2 pe = f2(0.f, 0.f), px = pe, py = pe, pz = pe;
-    for (int v = 0; v < maxL; ++v) {
-        const bool ok = v < L;
-        const bool inA = v < LA;
-        const int j = v + (inA ? sA : offB);
-        const float2 q = __ldg(&rec[ok ? j : kl]);
+    auto eval = [&](const float2& q, int j, bool ok, bool inA) {
         bool ma = ok && useA, mb = ok && useB;
         if (OWN) {
             ma = ma && j != ka;
@@ -517,6 +513,17 @@ __device__ __forceinline__ void mix_walk_pass2(const float2* __restrict__ rec, i
         py = __ffma2_rn(fsn, dy, py);
         pz = __ffma2_rn(fsn, dz, pz);
         a.np += (unsigned)ia + (unsigned)ib;
+    };
+    // two candidates per step: both records are loaded before either is evaluated
+    for (int v = 0; v < maxL; v += 2) {
+        const int v1 = v + 1;
+        const bool ok0 = v < L, ok1 = v1 < L;
+        const bool inA0 = v < LA, inA1 = v1 < LA;
+        const int j0 = v + (inA0 ? sA : offB), j1 = v1 + (inA1 ? sA : offB);
+        const float2 q0 = __ldg(&rec[ok0 ? j0 : kl]);
+        const float2 q1 = __ldg(&rec[ok1 ? j1 : kl]);
+        eval(q0, j0, ok0, inA0);
+        eval(q1, j1, ok1, inA1);
     }
     two_sum_add2(a.se, a.ce, pe);
     two_sum_add2(a.sx, a.cx, f2(-px.x, -px.y));
@@ -592,7 +599,7 @@ __device__ __forceinline__ void mix_passes2(const float2* __restrict__ rec, int 
     }
 }
 
-__global__ void __launch_bounds__(kMixThreads, 8) k_pair_mixed_pass2(GridDev g, MixParams mp,
+__global__ void __launch_bounds__(kMixThreads, 6) k_pair_mixed_pass2(GridDev g, MixParams mp,
                                                                      const float2* __restrict__ rec,
                                                                      const int* __restrict__ cs,
                                                                      const int* __restrict__ off, int n,
