@@ -128,7 +128,7 @@ extern "C" lj_status lj_set_stream(lj_ctx* c, void* stream) {
 }
 
 extern "C" lj_status lj_set_tuning(lj_ctx* c, const lj_tuning* t) {
-    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 11) return LJ_EINVAL;
+    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 10) return LJ_EINVAL;
     c->tuning = *t;
     return LJ_OK;
 }

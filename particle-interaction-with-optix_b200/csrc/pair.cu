@@ -137,7 +137,6 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
             case 8: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 3, energy, force, totals, kb, ke);
             case 9: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 4, energy, force, totals, kb, ke);
             case 10: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 5, energy, force, totals, kb, ke);
-            case 11: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 6, energy, force, totals, kb, ke);
             case 6: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 1, energy, force, totals, kb, ke);
             case 5: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 0, energy, force, totals, kb, ke);
             case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);

@@ -112,8 +112,7 @@ __global__ void __launch_bounds__(256) k_split_soa(const float4* __restrict__ p,
 lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                            const int* cs, const int* off, int mode, float* energy, float* force,
                            lj_totals* totals, int kb, int ke) {
-    const int threads = mode == 6 ? 64 : kPassThreads;
-    const int per_block = mode >= 3 ? 2 * threads : threads;
+    const int per_block = mode >= 3 ? 2 * kPassThreads : kPassThreads;
     const int blocks = (ke - kb + per_block - 1) / per_block;
     const size_t need = 256 + (size_t)blocks * sizeof(Partial);
     if (need > ctx->red_bytes) {
@@ -127,8 +126,7 @@ lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, 
     const GridDev gd = to_dev(*g);
     if (mode >= 3) {
         auto kern = mode == 3 ? k_pair_pass2<1, false> : (mode == 4 ? k_pair_pass2<8, false> : k_pair_pass2<8, true>);
-        if (mode == 6) kern = k_pair_pass2<16, true, 64>;
-        kern<<<blocks, threads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force, part, counter,
+        kern<<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force, part, counter,
                                                        totals, ctx->d_status);
     } else if (mode == 2) {
         const int ld = (n + 2 + 63) & ~63;
