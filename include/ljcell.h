@@ -242,7 +242,9 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  * particles whose windows hold it are unspecified under 5-10. */
 typedef struct {
     int pair_kernel;
-    int reserved[7];
+    int scatter_passes; /* binning scatter in this many passes over cell ranges (0 = one pass per
+                           56 MiB of scattered records, so each pass's writes meet in L2); 1-8 */
+    int reserved[6];
 } lj_tuning;
 
 LJ_API lj_status lj_set_tuning(lj_ctx* ctx, const lj_tuning* t);

@@ -128,7 +128,8 @@ extern "C" lj_status lj_set_stream(lj_ctx* c, void* stream) {
 }
 
 extern "C" lj_status lj_set_tuning(lj_ctx* c, const lj_tuning* t) {
-    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 10) return LJ_EINVAL;
+    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 10 || t->scatter_passes < 0 || t->scatter_passes > 8)
+        return LJ_EINVAL;
     c->tuning = *t;
     return LJ_OK;
 }

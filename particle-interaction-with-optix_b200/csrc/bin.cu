@@ -207,10 +207,13 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const int* __restrict__ c
 // write out of bounds.
 // Four particles per thread per round, all loads issued before the stores: the kernel is bound by
 // the latency of the offset gather and of the scattered 16-byte writes, not by bandwidth.
+// Only particles of cells [c_lo, c_hi) move: bin_finish runs it in passes over cell ranges whose
+// slots span a region that fits in L2, so the scattered 16-byte records of a cell meet there and
+// leave L2 as whole lines instead of as partial sectors.
 __global__ void __launch_bounds__(256) k_scatter(const float* __restrict__ x, const float* __restrict__ y,
                                                  const float* __restrict__ z, int stride, int n,
                                                  const int2* __restrict__ ct, const int* __restrict__ offsets,
-                                                 float4* __restrict__ tmp, unsigned* status) {
+                                                 float4* __restrict__ tmp, unsigned* status, int c_lo, int c_hi) {
     constexpr int U = 4;
     const long long step = (long long)gridDim.x * blockDim.x;
     for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * step) {
@@ -222,18 +225,20 @@ __global__ void __launch_bounds__(256) k_scatter(const float* __restrict__ x, co
         }
         long long slot[U];
         float px[U], py[U], pz[U];
+        bool mine[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const long long i = i0 + u * step;
-            slot[u] = i < n ? (long long)__ldg(&offsets[c[u].x]) + c[u].y : -1;
-            px[u] = i < n ? __ldg(&x[i * stride]) : 0.f;
-            py[u] = i < n ? __ldg(&y[i * stride]) : 0.f;
-            pz[u] = i < n ? __ldg(&z[i * stride]) : 0.f;
+            mine[u] = i < n && c[u].x >= c_lo && c[u].x < c_hi;
+            slot[u] = mine[u] ? (long long)__ldg(&offsets[c[u].x]) + c[u].y : -1;
+            px[u] = mine[u] ? __ldg(&x[i * stride]) : 0.f;
+            py[u] = mine[u] ? __ldg(&y[i * stride]) : 0.f;
+            pz[u] = mine[u] ? __ldg(&z[i * stride]) : 0.f;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const long long i = i0 + u * step;
-            if (i >= n) continue;
+            if (!mine[u]) continue;
             if (slot[u] >= 0 && slot[u] < n)
                 tmp[slot[u]] = make_float4(px[u], py[u], pz[u], __int_as_float((int)i));
             else
@@ -270,6 +275,7 @@ __device__ __forceinline__ void emit(const SortOut& o, long long slot, float4 r,
     if (o.sidx) o.sidx[slot] = __float_as_int(r.w);
 }
 
+constexpr long long kScatterRegion = 56LL << 20;  // bytes of tmp4 one scatter pass writes (L2 holds 126 MB)
 constexpr int kRankMax = 512;    // cells up to this size are ranked record by record
 constexpr int kLargeCapMin = 4096;
 
@@ -558,9 +564,16 @@ lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const flo
     cudaStream_t st = ctx->stream;
     if ((s = launch_scan(ctx, counts, nc, offsets)) != LJ_OK) return s;
     if (n > 0) {
-        k_scatter<<<grid_for(ctx, n, 256), 256, 0, st>>>(x, y, z, stride, n, ctx->cell_ticket, offsets, ctx->tmp4,
-                                                         ctx->d_status);
-        if ((s = last_launch_status()) != LJ_OK) return s;
+        // passes: the tuning's scatter_passes, else enough that each pass writes about kScatterRegion bytes
+        long long passes = ctx->tuning.scatter_passes;
+        if (passes <= 0) passes = ((long long)n * (long long)sizeof(float4) + kScatterRegion - 1) / kScatterRegion;
+        passes = std::max(1LL, std::min(passes, std::min(8LL, nc)));
+        for (long long q = 0; q < passes; ++q) {
+            const int c_lo = (int)(nc * q / passes), c_hi = (int)(nc * (q + 1) / passes);
+            k_scatter<<<grid_for(ctx, n, 256), 256, 0, st>>>(x, y, z, stride, n, ctx->cell_ticket, offsets,
+                                                             ctx->tmp4, ctx->d_status, c_lo, c_hi);
+            if ((s = last_launch_status()) != LJ_OK) return s;
+        }
     }
     SortOut so{reinterpret_cast<float4*>(sorted_xyzi), sorted_cell, nullptr, nullptr, nullptr, nullptr};
     if (sorted) {
@@ -843,7 +856,7 @@ extern "C" lj_status lj_reorder(lj_ctx* ctx, int n, float* points, float radius)
     if ((s = last_launch_status()) != LJ_OK) return s;
     if ((s = launch_scan(ctx, counts, nkeys, offsets)) != LJ_OK) return s;
     k_scatter<<<grid_for(ctx, n, 256), 256, 0, st>>>(points, points + 1, points + 2, 4, n, ctx->cell_ticket, offsets,
-                                                     ctx->tmp4, ctx->d_status);
+                                                     ctx->tmp4, ctx->d_status, 0, INT_MAX);
     if ((s = last_launch_status()) != LJ_OK) return s;
     SortOut so{sorted, keys, nullptr, nullptr, nullptr, nullptr};
     const int lcap = (int)ctx->large_cap;

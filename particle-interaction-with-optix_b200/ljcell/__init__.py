@@ -60,7 +60,7 @@ class Tuning(C.Structure):
     """lj_tuning: implementation choices (pair_kernel 0 default, 1 direct with shared-memory windows,
     2 direct with register windows, 3 direct with compaction, 4 tiled)."""
 
-    _fields_ = [("pair_kernel", C.c_int), ("reserved", C.c_int * 7)]
+    _fields_ = [("pair_kernel", C.c_int), ("scatter_passes", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class System(C.Structure):
@@ -250,9 +250,10 @@ class Context:
     def sync(self):
         _check(_lib.lj_sync(self._h), "lj_sync")
 
-    def set_tuning(self, pair_kernel: int = 0):
+    def set_tuning(self, pair_kernel: int = 0, scatter_passes: int = 0):
         t = Tuning()
         t.pair_kernel = pair_kernel
+        t.scatter_passes = scatter_passes
         _check(_lib.lj_set_tuning(self._h, C.byref(t)), "lj_set_tuning")
 
     def autotune_compute(self, g: Grid, p: Params, b: Binned):
@@ -266,7 +267,7 @@ class Context:
     def get_tuning(self) -> dict:
         t = Tuning()
         _check(_lib.lj_get_tuning(self._h, C.byref(t)), "lj_get_tuning")
-        return {"pair_kernel": t.pair_kernel}
+        return {"pair_kernel": t.pair_kernel, "scatter_passes": t.scatter_passes}
 
     # ------------------------------------------------------------ generation
     def _gen_out(self, n, want_soa, want_aos):

@@ -358,3 +358,17 @@ def test_autotune_compute_picks_a_kernel_and_keeps_results(torch_cuda, ctx):
     ctx.sync()
     ctx.set_tuning(0)
     assert ljcell.totals_from_tensor(tot)["pairs"] == O.config_forces(og, ob, rc).pairs
+
+
+@pytest.mark.parametrize("passes", [1, 2, 3, 8])
+@pytest.mark.parametrize("name", ["uniform_c1", "shell", "clustered"])
+def test_bin_scatter_passes_bit_exact(torch_cuda, ctx, name, passes):
+    """The binning scatter split into passes over cell ranges gives the oracle's binning bit for bit."""
+    ctx.set_tuning(0, passes)
+    try:
+        (x, y, z), g, og, b, ob, _ = bin_both(torch_cuda, ctx, name, 1)
+    finally:
+        ctx.set_tuning(0)
+    np.testing.assert_array_equal(np_(b.offsets), ob.offsets)
+    np.testing.assert_array_equal(np_(b.xyzi)[:len(x), 3].view(np.int32), ob.perm)
+    np.testing.assert_array_equal(np_(b.cell)[:len(x)], ob.cell_sorted)
