@@ -47,6 +47,13 @@ KERNEL_NAMES = {1: "k_pair_config", 2: "k_pair_direct<false>", 3: "k_pair_direct
                 9: "k_pair_pass2<8, false>", 10: "k_pair_pass2<8, true>"}
 # launches of the pair stage per lj_compute call (kernel 7 first copies x, y, z to SoA arrays)
 PAIR_LAUNCHES = {7: 2}
+SCATTER_REGION = 56 << 20   # bytes of scattered records per binning scatter pass (the library's default)
+
+
+def bin_launches(n: int, ncells: int) -> int:
+    """Kernels one lj_bin launches: count, scan, the scatter passes, rank, large-cell sort."""
+    passes = max(1, min(8, ncells, -(-16 * n // SCATTER_REGION)))
+    return 4 + passes
 
 CONFIGS = {
     "c1": dict(workload="uniform 100k, rc=0.05", n=100_000, dist="uniform", lo=(0, 0, 0), hi=(1, 1, 1), rc=0.05),
@@ -368,7 +375,7 @@ def run_ours(args, cfg):
                                         "SM clock; MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
                          "algorithmic_flops": algo_flops},
             "e2e": e2e,
-            "gpu_launches": (5 + PAIR_LAUNCHES.get(pair_kernel, 1)) * K,
+            "gpu_launches": (bin_launches(n, g.ncells) + PAIR_LAUNCHES.get(pair_kernel, 1)) * K,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         }
         if cpu:
