@@ -388,6 +388,24 @@ LJ_API lj_status lj_simulate_host(lj_ctx* ctx, const lj_grid* g, const lj_params
                            const float* hy, const float* hz, float* h_energy, float* h_force, int* h_index,
                            lj_totals* h_totals);
 
+/* The same step without the final synchronisation, for a caller that runs
+ * steps back to back (no counterpart in the reference): the call returns once
+ * the work is queued, and consecutive calls overlap -- the next call's
+ * positions go up on an upload stream while the previous call's results come
+ * down on the copy stream (PCIe carries both directions at once).  Two device
+ * buffer sets in the context are used in turn.  Host buffers must be pinned
+ * for the copies to overlap; the caller must leave the input buffers unchanged,
+ * keep every output buffer and h_totals valid, and not read them until
+ * lj_simulate_host_wait returns (h_totals is written by that call, from pinned
+ * staging in the context: at most 64 calls are staged, a 65th first waits for
+ * the queued ones).  Errors recorded by kernels are reported by
+ * lj_simulate_host_wait. */
+LJ_API lj_status lj_simulate_host_async(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* hx,
+                                        const float* hy, const float* hz, float* h_energy, float* h_force,
+                                        int* h_index, lj_totals* h_totals);
+/* Waits for every lj_simulate_host_async call queued so far, then as lj_sync. */
+LJ_API lj_status lj_simulate_host_wait(lj_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

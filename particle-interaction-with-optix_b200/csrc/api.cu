@@ -112,11 +112,22 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->soa);
     cudaFree(c->reorder);
     cudaFree(c->step);
+    if (c->e2ea_ready) {
+        cudaStreamSynchronize(c->up_stream);
+        for (int i = 0; i < 9; ++i) cudaEventDestroy(c->e2ea_ev[i]);
+        cudaStreamDestroy(c->up_stream);
+    }
+    if (c->e2ea_tot) {
+        if (c->e2e_ready) cudaStreamSynchronize(c->copy_stream);
+        cudaFreeHost(c->e2ea_tot);
+    }
     if (c->e2e_ready) {
         cudaStreamSynchronize(c->copy_stream);
         for (int i = 0; i < 8; ++i) cudaEventDestroy(c->e2e_ev[i]);
         cudaStreamDestroy(c->copy_stream);
     }
+    cudaFree(c->e2ea[0]);
+    cudaFree(c->e2ea[1]);
     delete c;
     return LJ_OK;
 }
@@ -305,5 +316,160 @@ extern "C" lj_status lj_simulate_host(lj_ctx* c, const lj_grid* g, const lj_para
         cudaMemcpyAsync(h_totals, dtot + kE2EChunks, sizeof(lj_totals), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return LJ_ECUDA;
     if (cudaStreamSynchronize(cp) != cudaSuccess) return LJ_ECUDA;
+    return lj_sync(c);
+}
+
+namespace ljc {
+
+constexpr int kE2EAPending = 64;  // queued lj_simulate_host_async calls whose totals await the wait call
+
+// Copies the staged totals of the queued calls to their callers (after the copy stream is drained).
+void e2ea_deliver(lj_ctx* c) {
+    for (int i = 0; i < c->e2ea_pending; ++i)
+        if (c->e2ea_dst[i]) *c->e2ea_dst[i] = c->e2ea_tot[i];
+    c->e2ea_pending = 0;
+}
+
+lj_status e2ea_setup(lj_ctx* c) {
+    if (c->e2ea_ready) return LJ_OK;
+    if (cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking) != cudaSuccess) return LJ_ECUDA;
+    for (int i = 0; i < 9; ++i)
+        if (cudaEventCreateWithFlags(&c->e2ea_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            for (int j = 0; j < i; ++j) cudaEventDestroy(c->e2ea_ev[j]);
+            cudaStreamDestroy(c->up_stream);
+            c->up_stream = nullptr;
+            return LJ_ECUDA;
+        }
+    // both slots start free
+    for (int i = 0; i < 2; ++i)
+        if (cudaEventRecord(c->e2ea_ev[i], c->up_stream) != cudaSuccess) return LJ_ECUDA;
+    // totals come back into pinned memory (a copy into pageable memory would make the call wait for
+    // the whole step); lj_simulate_host_wait hands them to the caller
+    if (cudaMallocHost(reinterpret_cast<void**>(&c->e2ea_tot), kE2EAPending * sizeof(lj_totals)) != cudaSuccess) {
+        c->e2ea_tot = nullptr;
+        return LJ_ENOMEM;
+    }
+    c->e2ea_pending = 0;
+    c->e2ea_ready = true;
+    return LJ_OK;
+}
+
+}  // namespace ljc
+
+extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx,
+                                            const float* hy, const float* hz, float* h_energy, float* h_force,
+                                            int* h_index, lj_totals* h_totals) {
+    if (!c || !g || !p || n < 0 || (n > 0 && (!hx || !hy || !hz))) return LJ_EINVAL;
+    if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
+    if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;
+    DeviceScope scope(c->device);
+    if (!scope.ok) return LJ_ECUDA;
+    const long long nc = (long long)g->dim[0] * g->dim[1] * g->dim[2];
+    if (nc < 1 || nc > 2147483646LL) return LJ_EINVAL;
+    lj_status s = e2e_setup(c);
+    if (s != LJ_OK) return s;
+    if ((s = e2ea_setup(c)) != LJ_OK) return s;
+    if (c->e2ea_pending == kE2EAPending) {  // staging full: drain the queued calls first
+        if (cudaStreamSynchronize(c->copy_stream) != cudaSuccess) return LJ_ECUDA;
+        e2ea_deliver(c);
+    }
+    const int slot = c->e2ea_slot;
+    cudaStream_t st = c->stream, cp = c->copy_stream, up = c->up_stream;
+    cudaEvent_t* ev = c->e2ea_ev;
+    // Nothing may touch this slot's buffers (grown or not) before its last download is done.
+    if (cudaStreamWaitEvent(up, ev[slot], 0) != cudaSuccess || cudaStreamWaitEvent(st, ev[slot], 0) != cudaSuccess)
+        return LJ_ECUDA;
+    const size_t N = (size_t)(n > 0 ? n : 1);
+    auto upb = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t b_pos = upb(3 * N * sizeof(float));
+    const size_t b_cnt = upb((size_t)nc * sizeof(int));
+    const size_t b_off = upb(((size_t)nc + 1) * sizeof(int));
+    const size_t b_x4 = upb(N * 16);
+    const size_t b_cell = upb(N * sizeof(int));
+    const size_t b_e = upb(N * sizeof(float));
+    const size_t b_f = upb(3 * N * sizeof(float));
+    const size_t b_idx = upb(N * sizeof(int));
+    const size_t b_tot = upb((kE2EChunks + 1) * sizeof(lj_totals));
+    const size_t need = b_pos + b_cnt + b_off + b_x4 + b_cell + b_e + b_f + b_idx + b_tot;
+    if (need > c->e2ea_bytes[slot]) {
+        // a grown slot: wait for its previous download on the host before freeing it
+        if (cudaEventSynchronize(ev[slot]) != cudaSuccess) return LJ_ECUDA;
+        if ((s = grow(&c->e2ea[slot], &c->e2ea_bytes[slot], need)) != LJ_OK) return s;
+    }
+    char* base = static_cast<char*>(c->e2ea[slot]);
+    float* dpos = reinterpret_cast<float*>(base);
+    base += b_pos;
+    int* dcnt = reinterpret_cast<int*>(base);
+    base += b_cnt;
+    int* doff = reinterpret_cast<int*>(base);
+    base += b_off;
+    float* dx4 = reinterpret_cast<float*>(base);
+    base += b_x4;
+    int* dcell = reinterpret_cast<int*>(base);
+    base += b_cell;
+    float* de = reinterpret_cast<float*>(base);
+    base += b_e;
+    float* df = reinterpret_cast<float*>(base);
+    base += b_f;
+    int* didx = reinterpret_cast<int*>(base);
+    base += b_idx;
+    lj_totals* dtot = reinterpret_cast<lj_totals*>(base);
+    // upload on its own stream: it overlaps the previous call's compute and downloads
+    const size_t pb = (size_t)n * sizeof(float);
+    if (n > 0 && (cudaMemcpyAsync(dpos, hx, pb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
+                  cudaMemcpyAsync(dpos + N, hy, pb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
+                  cudaMemcpyAsync(dpos + 2 * N, hz, pb, cudaMemcpyHostToDevice, up) != cudaSuccess))
+        return LJ_ECUDA;
+    if (cudaEventRecord(ev[2], up) != cudaSuccess || cudaStreamWaitEvent(st, ev[2], 0) != cudaSuccess)
+        return LJ_ECUDA;
+    lj_particles sorted{};
+    sorted.index = didx;
+    s = lj_bin(c, g, n, dpos, dpos + N, dpos + 2 * N, 1, LJ_ORDER_X, dcnt, doff, nullptr, &sorted, dx4, dcell);
+    if (s != LJ_OK) return s;
+    if (cudaEventRecord(ev[3], st) != cudaSuccess || cudaStreamWaitEvent(cp, ev[3], 0) != cudaSuccess)
+        return LJ_ECUDA;
+    if (n > 0 && h_index &&
+        cudaMemcpyAsync(h_index, didx, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, cp) != cudaSuccess)
+        return LJ_ECUDA;
+    const int chunks = (c->tuning.pair_kernel == 4 || n < kE2EChunks * 4096) ? 1 : kE2EChunks;
+    for (int k = 0; k < chunks; ++k) {
+        const int kb = (int)((long long)n * k / chunks), ke = (int)((long long)n * (k + 1) / chunks);
+        s = launch_pair_config(c, g, p, n, dx4, dcell, doff, LJ_ORDER_X, h_energy ? de : nullptr,
+                               h_force ? df : nullptr, dtot + k, kb, ke);
+        if (s != LJ_OK) return s;
+        if (ke == kb) continue;
+        if (cudaEventRecord(ev[4 + k], st) != cudaSuccess || cudaStreamWaitEvent(cp, ev[4 + k], 0) != cudaSuccess)
+            return LJ_ECUDA;
+        const size_t cb = (size_t)(ke - kb) * sizeof(float);
+        if (h_energy && cudaMemcpyAsync(h_energy + kb, de + kb, cb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
+            return LJ_ECUDA;
+        if (h_force &&
+            cudaMemcpyAsync(h_force + 3 * (size_t)kb, df + 3 * (size_t)kb, 3 * cb, cudaMemcpyDeviceToHost, cp) !=
+                cudaSuccess)
+            return LJ_ECUDA;
+    }
+    k_sum_totals<<<1, 1, 0, st>>>(dtot, chunks, dtot + kE2EChunks);
+    if ((s = last_launch_status()) != LJ_OK) return s;
+    if (cudaEventRecord(ev[8], st) != cudaSuccess || cudaStreamWaitEvent(cp, ev[8], 0) != cudaSuccess)
+        return LJ_ECUDA;
+    const int q = c->e2ea_pending;
+    if (cudaMemcpyAsync(c->e2ea_tot + q, dtot + kE2EChunks, sizeof(lj_totals), cudaMemcpyDeviceToHost, cp) !=
+        cudaSuccess)
+        return LJ_ECUDA;
+    c->e2ea_dst[q] = h_totals;
+    c->e2ea_pending = q + 1;
+    // the slot is free again once its downloads are done
+    if (cudaEventRecord(ev[slot], cp) != cudaSuccess) return LJ_ECUDA;
+    c->e2ea_slot = slot ^ 1;
+    return LJ_OK;
+}
+
+extern "C" lj_status lj_simulate_host_wait(lj_ctx* c) {
+    if (!c) return LJ_EINVAL;
+    DeviceScope scope(c->device);
+    if (!scope.ok) return LJ_ECUDA;
+    if (c->e2ea_ready && cudaStreamSynchronize(c->up_stream) != cudaSuccess) return LJ_ECUDA;
+    if (c->e2e_ready && cudaStreamSynchronize(c->copy_stream) != cudaSuccess) return LJ_ECUDA;
+    if (c->e2ea_ready) e2ea_deliver(c);
     return lj_sync(c);
 }

@@ -112,6 +112,18 @@ struct lj_ctx {
     cudaStream_t copy_stream;
     cudaEvent_t e2e_ev[8];
     bool e2e_ready;
+    // pipelined host-buffer steps (lj_simulate_host_async): two device buffer sets used in turn, an
+    // upload stream, and events: [0..1] slot free (its last download done), [2] upload done,
+    // [3] binning done, [4..7] pair chunks done, [8] totals done
+    void* e2ea[2];
+    size_t e2ea_bytes[2];
+    int e2ea_slot;
+    cudaStream_t up_stream;
+    cudaEvent_t e2ea_ev[9];
+    bool e2ea_ready;
+    lj_totals* e2ea_tot;         // pinned staging of the queued calls' totals (kE2EAPending entries)
+    lj_totals* e2ea_dst[64];     // caller's totals pointer of each queued call
+    int e2ea_pending;
 };
 
 namespace ljc {

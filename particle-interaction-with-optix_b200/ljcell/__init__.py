@@ -129,6 +129,9 @@ def _load() -> C.CDLL:
                                  vp, vp, vp, vp]),
         "lj_simulate_host": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
                                    C.POINTER(Totals)]),
+        "lj_simulate_host_async": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
+                                   C.POINTER(Totals)]),
+        "lj_simulate_host_wait": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -144,7 +147,8 @@ ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj
                "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_autotune_compute", "lj_batch_create",
                "lj_batch_destroy", "lj_batch_get_config", "lj_batch_grid", "lj_batch_run", "lj_batch_run_graph",
                "lj_batch_run_separate", "lj_batch_autotune", "lj_pack_mixed", "lj_compute_mixed",
-               "lj_test_scan_withheld_tile", "lj_reorder", "lj_step_verlet", "lj_simulate_host")
+               "lj_test_scan_withheld_tile", "lj_reorder", "lj_step_verlet", "lj_simulate_host",
+               "lj_simulate_host_async", "lj_simulate_host_wait")
 
 
 def lib() -> C.CDLL:
@@ -416,6 +420,29 @@ class Context:
         _check(_lib.lj_simulate_host(self._h, C.byref(g), C.byref(p), n, fp(hx), fp(hy), fp(hz), fp(energy),
                                      fp(force), fp(index), C.byref(tot)), "lj_simulate_host")
         return tot
+
+    def simulate_host_async(self, g: Grid, p: Params, hx: np.ndarray, hy: np.ndarray, hz: np.ndarray,
+                            energy: np.ndarray | None = None, force: np.ndarray | None = None,
+                            index: np.ndarray | None = None, totals=None):
+        """lj_simulate_host_async: queues one host-buffer step and returns; the arrays (pinned for the
+        copies to overlap) and the returned Totals must stay alive and untouched until
+        simulate_host_wait()."""
+        n = len(hx)
+        tot = totals if totals is not None else Totals()
+        fp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        # the library writes into these at lj_simulate_host_wait: keep them alive until then
+        if not hasattr(self, "_pending"):
+            self._pending = []
+        self._pending.append((tot, hx, hy, hz, energy, force, index))
+        _check(_lib.lj_simulate_host_async(self._h, C.byref(g), C.byref(p), n, fp(hx), fp(hy), fp(hz), fp(energy),
+                                           fp(force), fp(index), C.byref(tot)), "lj_simulate_host_async")
+        return tot
+
+    def simulate_host_wait(self):
+        try:
+            _check(_lib.lj_simulate_host_wait(self._h), "lj_simulate_host_wait")
+        finally:
+            self._pending = []
 
 
 def totals_from_tensor(tot) -> dict:

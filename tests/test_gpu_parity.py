@@ -372,3 +372,35 @@ def test_bin_scatter_passes_bit_exact(torch_cuda, ctx, name, passes):
     np.testing.assert_array_equal(np_(b.offsets), ob.offsets)
     np.testing.assert_array_equal(np_(b.xyzi)[:len(x), 3].view(np.int32), ob.perm)
     np.testing.assert_array_equal(np_(b.cell)[:len(x)], ob.cell_sorted)
+
+
+def test_simulate_host_async_matches_one_call(torch_cuda, ctx):
+    """Back-to-back lj_simulate_host_async calls (two device buffer sets used in turn, uploads on their
+    own stream) give, per call, the outputs of lj_simulate_host on the same inputs, bit for bit."""
+    import ljcell
+
+    torch = torch_cuda
+    (x, y, z), (lo, hi), rc = case_positions("uniform_c1")
+    n = len(x)
+    g = ljcell.grid_from_box(lo, hi, rc)
+    p = ljcell.params(rc)
+    inputs = [(x, y, z), (y.copy(), z.copy(), x.copy()), (z.copy(), x.copy(), y.copy())]
+
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+
+    outs = []
+    for (a, b, c) in inputs:
+        hp = [pinned(n, torch.float32) for _ in range(3)]
+        for h, v in zip(hp, (a, b, c)):
+            h[:] = v
+        outs.append((hp, pinned(n, torch.float32), pinned((n, 3), torch.float32), pinned(n, torch.int32)))
+    tots = [ctx.simulate_host_async(g, p, *hp, he, hf, hi_) for hp, he, hf, hi_ in outs]
+    ctx.simulate_host_wait()
+    for (hp, he, hf, hi_), t in zip(outs, tots):
+        re, rf, ri = np.empty(n, np.float32), np.empty((n, 3), np.float32), np.empty(n, np.int32)
+        rt = ctx.simulate_host(g, p, *hp, re, rf, ri)
+        np.testing.assert_array_equal(he, re)
+        np.testing.assert_array_equal(hf, rf)
+        np.testing.assert_array_equal(hi_, ri)
+        assert t.pairs == rt.pairs and t.energy == rt.energy
