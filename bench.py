@@ -549,8 +549,10 @@ def run_extras(ctx, dev, flush, peak_tflops):
 
 
 def run_e2e(ctx, g, p, x, y, z, n, K, ws, dev, total_pairs, pairs):
-    """Same metric through lj_simulate_host(): pinned host positions in,
-    energy / force / index out, copies inside the timed region."""
+    """Same metric through the host-buffer entry: pinned host positions in,
+    energy / force / index out every step, copies inside the timed region;
+    steps back to back through lj_simulate_host_async(), one
+    lj_simulate_host() call timed beside them."""
     import torch
 
     hx, hy, hz = (torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(3))
