@@ -65,6 +65,12 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
+// r^-2 of a candidate pair, or an exact 0 when it does not interact (rcp.approx.ftz(+inf) = +0):
+// one reciprocal on every lane, with no branch around it.
+__device__ __forceinline__ float rcp_hit(bool hit, float r2) {
+    return rcp_approx(hit ? r2 : __int_as_float(0x7f800000));
+}
+
 // Warp sums.
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

@@ -91,13 +91,30 @@ __device__ void reduce_totals(double e, double w, unsigned long long np, Partial
     __syncthreads();
     if (!s_last) return;
     __threadfence();
+    // The last block reads every block's partial: eight independent L2 loads in flight per thread,
+    // each thread's share in a fixed order, so the totals are the same on every run.
     double te = 0, tw = 0;
     unsigned long long tp = 0;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-        const volatile Partial* q = part + b;
-        te += q->e;
-        tw += q->w;
-        tp += q->p;
+    const unsigned nb = gridDim.x;
+    for (unsigned b0 = 0; b0 < nb; b0 += 8 * blockDim.x) {
+        Partial q[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const unsigned b = b0 + u * blockDim.x + threadIdx.x;
+            q[u] = Partial{0.0, 0.0, 0ULL, 0ULL};
+            if (b < nb) {
+                const double2 ew = __ldcg(reinterpret_cast<const double2*>(part + b));
+                q[u].e = ew.x;
+                q[u].w = ew.y;
+                q[u].p = __ldcg(&part[b].p);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            te += q[u].e;
+            tw += q[u].w;
+            tp += q[u].p;
+        }
     }
     te = warp_sum(te);
     tw = warp_sum(tw);

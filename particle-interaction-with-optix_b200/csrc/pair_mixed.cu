@@ -364,7 +364,7 @@ __device__ __forceinline__ void mix_walk_pass(const float2* __restrict__ rec, in
         const float2 dz = __fadd2_rn(f2(u0.y, u1.y), f2(a0 ? ntzA : ntzB, a1 ? ntzA : ntzB));
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const bool in0 = m0 && r2.x < rc2, in1 = m1 && r2.y < rc2;
-        const float2 ir2 = f2(in0 ? rcp_approx(r2.x) : 0.f, in1 ? rcp_approx(r2.y) : 0.f);
+        const float2 ir2 = f2(rcp_hit(in0, r2.x), rcp_hit(in1, r2.y));
         const float2 s2n = __fmul2_rn(nsig2, ir2);
         const float2 s4 = __fmul2_rn(s2n, s2n);
         const float2 ns6 = __fmul2_rn(s4, s2n);
@@ -500,7 +500,7 @@ __device__ __forceinline__ void mix_walk_pass2(const float2* __restrict__ rec, i
         const float2 dz = __fadd2_rn(f2(u.y, u.y), inA ? ntzA : ntzB);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const bool ia = ma && r2.x < rc2, ib = mb && r2.y < rc2;
-        const float2 ir2 = f2(ia ? rcp_approx(r2.x) : 0.f, ib ? rcp_approx(r2.y) : 0.f);
+        const float2 ir2 = f2(rcp_hit(ia, r2.x), rcp_hit(ib, r2.y));
         const float2 s2n = __fmul2_rn(nsig2, ir2);
         const float2 s4 = __fmul2_rn(s2n, s2n);
         const float2 ns6 = __fmul2_rn(s4, s2n);

@@ -67,7 +67,7 @@ __device__ __forceinline__ void walk_pass(const float4* __restrict__ p, int k, i
             const float2 dz = __fadd2_rn(make_float2(q0.z, q1.z), npz);
             const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
             const bool in0 = m0 && r2.x < rc2, in1 = m1 && r2.y < rc2;
-            const float2 ir2 = make_float2(in0 ? rcp_approx(r2.x) : 0.f, in1 ? rcp_approx(r2.y) : 0.f);
+            const float2 ir2 = make_float2(rcp_hit(in0, r2.x), rcp_hit(in1, r2.y));
             const float2 s2n = __fmul2_rn(nsig2, ir2);  // -s2
             const float2 s4 = __fmul2_rn(s2n, s2n);     // s2 * s2
             const float2 ns6 = __fmul2_rn(s4, s2n);     // -s6
@@ -147,7 +147,7 @@ __device__ __forceinline__ void walk_pass_soa(const float2* __restrict__ x2, con
         const float2 dz = __fadd2_rn(qz, npz);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const bool in0 = m0 && r2.x < rc2, in1 = m1 && r2.y < rc2;
-        const float2 ir2 = make_float2(in0 ? rcp_approx(r2.x) : 0.f, in1 ? rcp_approx(r2.y) : 0.f);
+        const float2 ir2 = make_float2(rcp_hit(in0, r2.x), rcp_hit(in1, r2.y));
         const float2 s2n = __fmul2_rn(nsig2, ir2);
         const float2 s4 = __fmul2_rn(s2n, s2n);
         const float2 ns6 = __fmul2_rn(s4, s2n);
@@ -274,7 +274,7 @@ __device__ __forceinline__ void eval2(const float4& q, int j, bool ok, bool useA
     const float2 dz = __fadd2_rn(make_float2(q.z, q.z), nz);
     const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
     const bool ia = ma && r2.x < rc2, ib = mb && r2.y < rc2;
-    const float2 ir2 = make_float2(ia ? rcp_approx(r2.x) : 0.f, ib ? rcp_approx(r2.y) : 0.f);
+    const float2 ir2 = make_float2(rcp_hit(ia, r2.x), rcp_hit(ib, r2.y));
     const float2 s2n = __fmul2_rn(nsig2, ir2);
     const float2 s4 = __fmul2_rn(s2n, s2n);
     const float2 ns6 = __fmul2_rn(s4, s2n);
