@@ -158,9 +158,13 @@ LJ_API lj_status lj_exclusive_scan(lj_ctx* ctx, const int* counts, long long nce
  * the library holds until the process exits.
  *   - ncells <= 67,108,864 (2^26); larger returns LJ_EUNSUPPORTED.
  *   - No cudaMalloc / cudaFree and no allocating library call.
- *   - The first call on each device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture begins.
+ *   - Every call looks up the array's device address on the current device
+ *     (cudaGetSymbolAddress, which allocates nothing), so a device reset
+ *     between calls is harmless; the first call on a device may load the
+ *     library's device code there, so make it before any stream capture
+ *     begins.
+ *   - `stream` must belong to the current device (LJ_EINVAL otherwise): the
+ *     array used is the current device's.
  *   - Every call uses the same array: calls that may overlap on the GPU
  *     (different streams, no ordering between them) race and must not be
  *     issued.  Each call clears the part it uses before the scan.
@@ -342,6 +346,9 @@ LJ_API lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params
  * its first tile withheld, so every bounded look-back wait gives up; the next
  * lj_sync returns LJ_ETIMEOUT and the context stays usable.  ncells > 4096. */
 LJ_API lj_status lj_test_scan_withheld_tile(lj_ctx* ctx, const int* counts, long long ncells, int* offsets);
+/* The same failure path for lj_exclusive_scan_noalloc, on its fixed array: every bounded look-back
+ * wait gives up and the call marks its result invalid with offsets[ncells] = -1.  ncells > 4096. */
+LJ_API lj_status lj_test_scan_noalloc_withheld_tile(const int* counts, long long ncells, int* offsets, void* stream);
 
 /* ------------------------------------------------------------- time step
  * One velocity-Verlet step of the truncated law with rebinning (no stage of
@@ -367,14 +374,18 @@ LJ_API lj_status lj_step_verlet(lj_ctx* ctx, const lj_grid* g, const lj_params* 
  * Replaces reorder(N, points, radius) (SDK/optixMultiSphereAABB/sort.cu:29-41,
  * key kernel count_per_cell :7-18): sorts n float4 points in place by the key
  * of their cell and stores the key in .w as float.  width = int(1.0f/radius);
- * key = int(x/radius) + int(y/radius)*width + int(z/radius)*width*width with
- * IEEE float division, truncation and int arithmetic, as the reference.
- * Points with equal .w keep their input order (the reference's thrust::sort
- * leaves that order unspecified).  points: device, 16-byte aligned.  The
- * domain is the reference's, coordinates in [0, 1]: a point whose key falls
- * outside it (or a NaN coordinate) is reported as LJ_ERANGE by lj_sync and
- * sorted as key 0.  width <= 512 (radius > 1/513), else LJ_EUNSUPPORTED.
- * Scratch is the context's; asynchronous on its stream. */
+ * key = int(x/radius) + int(y/radius)*width + int(z/radius)*width*width as
+ * the reference's own build computes it: its SDK compiles sort.cu with
+ * --use_fast_math, so the divisions are the fast single-precision division
+ * (which can put a coordinate within a couple of ulps of a cell face in the
+ * neighbouring cell, unlike IEEE division), truncated; the stored key is the
+ * exact integer sum rounded once to float, equal to the reference's
+ * contracted float sum.  Points with equal .w keep their input order (the
+ * reference's thrust::sort leaves that order unspecified).  points: device,
+ * 16-byte aligned.  The domain is the reference's, coordinates in [0, 1]: a
+ * point whose key falls outside it (or a NaN coordinate) is reported as
+ * LJ_ERANGE by lj_sync and sorted as key 0.  width <= 512 (radius > 1/513),
+ * else LJ_EUNSUPPORTED.  Scratch is the context's; asynchronous on its stream. */
 LJ_API lj_status lj_reorder(lj_ctx* ctx, int n, float* points, float radius);
 
 /* ------------------------------------------------------------- end to end

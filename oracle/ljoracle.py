@@ -387,12 +387,19 @@ def reorder(points: np.ndarray, radius: float) -> np.ndarray:
     """Restatement of the reference's reorder(N, points, radius)
     (SDK/optixMultiSphereAABB/sort.cu:29-41) and its key kernel count_per_cell
     (sort.cu:7-18): width = int(1.0f / radius) (:30); per point
-    cell = int(x / radius) per axis in float32 IEEE division and truncation
-    (:12-14); id = cell_x + cell_y * width + cell_z * width * width in int
-    (:15); .w = float(id) (:16); sort by .w ascending (:20-25, :38).  Points
-    of equal .w keep their input order (a stable sort): the reference's
-    thrust::sort leaves that order unspecified, so comparisons against the
-    reference itself use per-key sets.  Returns a new (n, 4) float32 array."""
+    cell = int(x / radius) per axis, truncated (:12-14); id = cell_x +
+    cell_y * width + cell_z * width * width (:15); .w = float(id) (:16); sort
+    by .w ascending (:20-25, :38).  The division here is IEEE float32; the
+    reference's own build (--use_fast_math) divides with the fast approximate
+    division, which puts a coordinate lying within a couple of ulps of a cell
+    face into the neighbouring cell now and then, so comparisons with this
+    restatement use points away from the faces, and the reference's sort.cu
+    built from source (sortref_keys, sortref_reorder) is the checker for the
+    rest.  The integer id rounded once to float equals the reference's float
+    sum as its compiler contracts it (fused multiply-adds).  Points of equal
+    .w keep their input order (a stable sort): the reference's thrust::sort
+    leaves that order unspecified, so comparisons against the reference
+    itself use per-key sets.  Returns a new (n, 4) float32 array."""
     p = np.ascontiguousarray(points, dtype=np.float32)
     r = np.float32(radius)
     width = int(np.float32(1.0) / r)
@@ -418,3 +425,47 @@ def verlet_drift(xyz: np.ndarray, vel: np.ndarray, force: np.ndarray, dt: float,
     v2 = (vel.astype(np.float32) + h * force.astype(np.float32)).astype(np.float32)
     x2 = (xyz.astype(np.float32) + np.float32(dt) * v2).astype(np.float32)
     return x2, v2, h
+
+
+# --------------------------------------------------------------------- reference spatial sort
+_SORTREF_SO = os.path.join(_HERE, "_ref", "libljsortref.so")
+_sortref = None
+
+
+def sortref_available() -> bool:
+    return os.path.exists(_SORTREF_SO)
+
+
+def _sortref_lib():
+    """The reference's sort.cu (reorder, count_per_cell) built from source with its own flags into
+    _ref/libljsortref.so (GPU)."""
+    global _sortref
+    if _sortref is None:
+        if not os.path.exists(_SORTREF_SO):
+            raise RuntimeError(f"reference sort harness missing: {_SORTREF_SO} (run `make -C oracle sortref`)")
+        r = C.CDLL(_SORTREF_SO)
+        r.ljsr_keys.restype = C.c_int
+        r.ljsr_keys.argtypes = [C.c_int, _f32p, C.c_float, _f32p]
+        r.ljsr_reorder.restype = C.c_int
+        r.ljsr_reorder.argtypes = [C.c_int, _f32p, C.c_float]
+        _sortref = r
+    return _sortref
+
+
+def sortref_keys(points: np.ndarray, radius: float) -> np.ndarray:
+    """The reference's key (.w after count_per_cell) of each (n, 4) float32 point, input order."""
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
+    keys = np.empty(len(pts), np.float32)
+    rc = _sortref_lib().ljsr_keys(len(pts), pts.reshape(-1), radius, keys)
+    if rc != 0:
+        raise RuntimeError(f"reference count_per_cell failed: {rc}")
+    return keys
+
+
+def sortref_reorder(points: np.ndarray, radius: float) -> np.ndarray:
+    """The reference's reorder(N, points, radius) on a copy of the (n, 4) float32 points."""
+    pts = np.array(points, np.float32).reshape(-1, 4)
+    rc = _sortref_lib().ljsr_reorder(len(pts), pts.reshape(-1), radius)
+    if rc != 0:
+        raise RuntimeError(f"reference reorder failed: {rc}")
+    return pts

@@ -14,7 +14,6 @@
 // instead of per particle).
 #include <algorithm>
 #include <climits>
-#include <mutex>
 
 #include "ljcell_internal.cuh"
 
@@ -681,24 +680,16 @@ constexpr size_t kNoAllocScratchBytes = 256 + (size_t)kNoAllocMaxTiles * sizeof(
 // [0, 4): tile counter; [4, 8): status word; [256, ...): tile states.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-static std::mutex g_noalloc_mutex;
-static void* g_noalloc_addr[kNoAllocMaxDevices];
-
-// Device address of the array on the current device, looked up once per device.
+// Device address of the array on the current device.  Looked up on every call (cudaGetSymbolAddress
+// allocates nothing): an address kept from an earlier call would go stale if the caller reset the
+// device in between.
 static lj_status noalloc_scratch(void** out) {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return LJ_ECUDA;
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-            cudaGetLastError();
-            return LJ_ECUDA;
-        }
-        g_noalloc_addr[dev] = p;
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+        cudaGetLastError();
+        return LJ_ECUDA;
     }
-    *out = g_noalloc_addr[dev];
+    *out = p;
     return LJ_OK;
 }
 
@@ -708,36 +699,64 @@ __global__ void k_noalloc_mark(const unsigned* status, int* offsets, long long n
     if (*status) offsets[n] = -1;
 }
 
-}  // namespace ljc
-
-extern "C" lj_status lj_exclusive_scan_noalloc(const int* counts, long long ncells, int* offsets, void* stream) {
+// The scan on the array.  withhold: tile 0 is never published (the tile counter starts at 1 and one
+// CTA fewer runs), so every bounded look-back wait gives up: the failure path, for tests.
+static lj_status noalloc_scan(const int* counts, long long ncells, int* offsets, void* stream, bool withhold) {
     if (ncells < 0 || !offsets || (ncells > 0 && !counts)) return LJ_EINVAL;
     if (ncells > kNoAllocMaxCells) return LJ_EUNSUPPORTED;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return LJ_ECUDA;
+    if (st) {  // the array resolved below is the current device's: the stream must belong to it
+        int sdev = -1;
+        if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) {
+            cudaGetLastError();
+            return LJ_EINVAL;
+        }
+        if (sdev != cur) return LJ_EINVAL;
+    }
     void* scratch = nullptr;
     lj_status s = noalloc_scratch(&scratch);
     if (s != LJ_OK) return s;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (ncells == 0) return cudaMemsetAsync(offsets, 0, sizeof(int), st) == cudaSuccess ? LJ_OK : LJ_ECUDA;
     const long long ntiles = (ncells + kScanTile - 1) / kScanTile;
+    if (withhold && ntiles < 2) return LJ_EINVAL;
     // the counter, status and the states this call uses must start at zero; the array keeps the last call's values
     const size_t used = 256 + (size_t)ntiles * sizeof(unsigned long long);
     if (cudaMemsetAsync(scratch, 0, used, st) != cudaSuccess) return LJ_ECUDA;
     unsigned* counter = static_cast<unsigned*>(scratch);
     unsigned* status = counter + 1;
     unsigned long long* states = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) + 256);
+    if (withhold) k_set_u32<<<1, 1, 0, st>>>(counter, 1u);
     const int vec_ok = ((reinterpret_cast<uintptr_t>(counts) | reinterpret_cast<uintptr_t>(offsets)) & 15) == 0;
-    k_scan<<<(unsigned)ntiles, kScanThreads, 0, st>>>(counts, offsets, ncells, ntiles, states, counter, vec_ok,
-                                                     status);
+    k_scan<<<(unsigned)(withhold ? ntiles - 1 : ntiles), kScanThreads, 0, st>>>(counts, offsets, ncells, ntiles,
+                                                                                 states, counter, vec_ok, status);
     if ((s = last_launch_status()) != LJ_OK) return s;
     k_noalloc_mark<<<1, 1, 0, st>>>(status, offsets, ncells);
     return last_launch_status();
 }
 
+}  // namespace ljc
+
+extern "C" lj_status lj_exclusive_scan_noalloc(const int* counts, long long ncells, int* offsets, void* stream) {
+    return noalloc_scan(counts, ncells, offsets, stream, false);
+}
+
+extern "C" lj_status lj_test_scan_noalloc_withheld_tile(const int* counts, long long ncells, int* offsets,
+                                                        void* stream) {
+    return noalloc_scan(counts, ncells, offsets, stream, true);
+}
+
 // ---------------------------------------------------------------- spatial sort (lj_reorder)
 // The operation of the reference's reorder() (SDK/optixMultiSphereAABB/sort.cu:29-41 with its key
 // kernel count_per_cell, :7-18): each float4 point gets the key of its cell, width = int(1 / radius),
-// id = int(x / radius) + int(y / radius) * width + int(z / radius) * width^2 (IEEE division,
-// truncation, int arithmetic), stored in .w as float, and the points are sorted by .w.  Here the sort
+// id = int(x / radius) + int(y / radius) * width + int(z / radius) * width^2, stored in .w as float,
+// and the points are sorted by .w.  The division is the one the reference's own build performs: its
+// SDK compiles sort.cu with --use_fast_math, so x / radius is the fast single-precision division
+// (__fdividef here; it and IEEE division can truncate to different cells for a coordinate within a
+// couple of ulps of a cell face).  The key is summed in exact integers: stored in .w (one rounding to
+// float) it equals the reference's float sum, which the compiler contracts into fused multiply-adds
+// (both checked against the reference built from source, on points next to cell faces too).  Here the sort
 // is a counting sort over the keys on the binning kernels: count with tickets, scan, ticket scatter
 // (k_scatter, reading x, y, z with stride 4), then a rank by original index within each key, so
 // points of equal .w keep their input order (the reference's thrust::sort leaves that order open).
@@ -754,9 +773,9 @@ struct ReorderKey {
 };
 
 __device__ __forceinline__ int reorder_key(const ReorderKey& rk, float x, float y, float z, bool& bad) {
-    const int cx = __float2int_rz(__fdiv_rn(x, rk.radius));
-    const int cy = __float2int_rz(__fdiv_rn(y, rk.radius));
-    const int cz = __float2int_rz(__fdiv_rn(z, rk.radius));
+    const int cx = __float2int_rz(__fdividef(x, rk.radius));
+    const int cy = __float2int_rz(__fdividef(y, rk.radius));
+    const int cz = __float2int_rz(__fdividef(z, rk.radius));
     const long long id = (long long)cx + (long long)cy * rk.width + (long long)cz * rk.width * rk.width;
     bad = !(x == x && y == y && z == z) || id < 0 || id > INT_MAX;
     const int kf = bad ? 0 : __float2int_rz(__int2float_rn((int)id));

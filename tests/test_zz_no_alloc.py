@@ -46,3 +46,27 @@ def test_noalloc_scan_rejects_too_many_cells(torch_cuda):
     t = torch.zeros(8, dtype=torch.int32, device="cuda")
     rc = ljcell.lib().lj_exclusive_scan_noalloc(_p(t), (1 << 26) + 1, _p(t), None)
     assert rc == ljcell.LJ_EUNSUPPORTED
+
+
+def test_noalloc_scan_timeout_path_then_recovers(torch_cuda):
+    """With tile 0 withheld every bounded look-back wait gives up (no fault, no hang): the call marks
+    its result invalid with offsets[n] = -1.  The next normal call clears the array's status word
+    and counter and returns the correct scan."""
+    torch = torch_cuda
+    import ljcell
+
+    n = 200_003
+    stream = torch.cuda.current_stream()
+    counts = torch.randint(0, 9, (n,), dtype=torch.int32, device="cuda")
+    out = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    rc = ljcell.lib().lj_test_scan_noalloc_withheld_tile(_p(counts), n, _p(out), C.c_void_p(stream.cuda_stream))
+    assert rc == ljcell.LJ_OK, ljcell.status_str(rc)
+    torch.cuda.synchronize()
+    assert int(out[-1]) == -1
+    out2 = torch.full((n + 1,), -7, dtype=torch.int32, device="cuda")
+    rc = ljcell.lib().lj_exclusive_scan_noalloc(_p(counts), n, _p(out2), C.c_void_p(stream.cuda_stream))
+    assert rc == ljcell.LJ_OK, ljcell.status_str(rc)
+    torch.cuda.synchronize()
+    ref = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    ref[1:] = torch.cumsum(counts.to(torch.int64), 0)
+    assert torch.equal(out2.to(torch.int64), ref)
