@@ -203,7 +203,12 @@ LJ_API lj_status lj_count_candidates(lj_ctx* ctx, const lj_grid* g, const int* o
  * k, summed over every particle of the clamped 27-cell stencil except itself,
  * with 4 eps ((s/r)^12 - (s/r)^6), eps = s = 1, r = sqrt(d.d + 1e-5) and no
  * cutoff test: replaces ComputeParticleInterationsParPartNoLoop
- * (cudaLJ.cu:299-341).  Device pointers from lj_bin. */
+ * (cudaLJ.cu:299-341).  s/r comes from the approximate reciprocal square
+ * root (at most 2 ulp) where the reference divides by an IEEE square root:
+ * each particle's energy is within about 3e-6 relative of the reference's law
+ * for stencils narrower than 1/sqrt(3) (the reference's own check allows
+ * 1e-5, cudaLJ.cu:246-250).  Any within-cell order.  Device pointers from
+ * lj_bin. */
 LJ_API lj_status lj_compute_compat(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi, const int* sorted_cell,
                             const int* offsets, float* v);
 

@@ -2,10 +2,12 @@
 //
 // k_pair_compat replaces ComputeParticleInterationsParPartNoLoop
 // (cudaLJ.cu:299-341) with the reference's law and stencil: every particle of
-// the clamped 27-cell block except itself, r = sqrt(d.d + 1e-5), IEEE sqrt and
-// division, 4 eps ((1/r)^12 - (1/r)^6) with eps = sigma = 1, no cutoff.  The 27
-// cells are read as 9 rows of 3 consecutive cells, contiguous in cell order,
-// and positions come as one float4 load instead of three scalar loads.
+// the clamped 27-cell block except itself, r = sqrt(d.d + 1e-5),
+// 4 eps ((1/r)^12 - (1/r)^6) with eps = sigma = 1, no cutoff; 1/r from the
+// approximate reciprocal square root, within the reference's own tolerance
+// (see the kernel).  Two targets per lane, the 27 cells read as 9 rows of 3
+// consecutive cells (contiguous in cell order) in lockstep passes, one float4
+// load per candidate shared by both targets.
 //
 // k_pair_config evaluates the truncated law with forces.  One thread per
 // sorted target particle.  For each of the 9 stencil rows it bounds the
@@ -20,6 +22,7 @@
 // reduced in FP64 / u64 per block and then by the last block in a fixed
 // order, so they are deterministic.
 #include <cfloat>
+#include <climits>
 
 #include "pair_common.cuh"
 
@@ -65,39 +68,183 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairPar
                                 (unsigned long long)np, part, counter, totals);
 }
 
+// ---------------------------------------------------------------- reference law (compat)
+// Lane m of a warp takes the consecutive sorted targets a = 2m and b = 2m + 1.  Every particle of a
+// target's clamped 27-cell stencil except itself is a partner (no cutoff), so its 9 rows of 3 cells
+// are walked whole.  When a and b sit in the same (y, z) row of cells (cxb >= cxa) their rows are the
+// same rows of cells shifted by cxb - cxa: each row is walked once over the union of the two ranges
+// and each candidate loaded once is evaluated for both targets in paired FP32, each target masked to
+// its own 3 cells and to j != itself.  The rows are taken in 5 passes, all lanes of a warp in
+// lockstep (the own row, then opposite rows paired), so the warp's loads fall on a few neighbouring
+// lines.  A lane whose targets lie in different rows walks a's rows, then, in a second round that only
+// warps holding such a lane take, b's.
+//
+// The law is the reference's, 4 eps ((s/r)^12 - (s/r)^6) with eps = s = 1 and
+// r = sqrt(d.d + 1e-5), with s/r taken from the approximate reciprocal square root (rsqrt.approx.ftz,
+// at most 2 ulp) where the reference divides 1 by an IEEE square root: (s/r)^12 then carries at most
+// about 12 * 2^-22 relative error, and every term is positive whenever r < 1 (always within a stencil
+// of cells narrower than 1/sqrt(3)), so a particle's energy stays within about 3e-6 of the
+// reference's law (the reference's own check allows 1e-5, cudaLJ.cu:246-250).  A masked candidate
+// gets r^2 = +inf, whose reciprocal square root is an exact 0: no branch.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Candidate q against targets (a, b) (minus their coordinates in nx, ny, nz); masks ma, mb.
+__device__ __forceinline__ void compat2(const float4& q, bool ma, bool mb, float2 nx, float2 ny, float2 nz,
+                                        float2& pot) {
+    const float inf = __int_as_float(0x7f800000);
+    const float2 dx = __fadd2_rn(make_float2(q.x, q.x), nx);
+    const float2 dy = __fadd2_rn(make_float2(q.y, q.y), ny);
+    const float2 dz = __fadd2_rn(make_float2(q.z, q.z), nz);
+    const float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const float2 r2 = __fadd2_rn(d2, make_float2(1e-5f, 1e-5f));
+    const float2 sdr = make_float2(rsqrt_approx(ma ? r2.x : inf), rsqrt_approx(mb ? r2.y : inf));
+    const float2 s2 = __fmul2_rn(sdr, sdr);
+    const float2 s4 = __fmul2_rn(s2, s2);
+    const float2 r6 = __fmul2_rn(s4, s2);
+    const float2 r12 = __fmul2_rn(r6, r6);
+    pot = __fadd2_rn(pot, __ffma2_rn(r6, make_float2(-1.0f, -1.0f), r12));  // r12 - r6, one rounding
+}
+
+// One window of a row for both targets: candidates [s, e); target a takes those below ea, target b
+// those from sb on (a's 3 cells start the union, b's end it).
+struct CompatRow {
+    int s, e, ea, sb;
+};
+
+// Row (dy, dz) of cell (cx, cy, cz) clamped to the grid: [s, e), the particles of cells cx-1..cx+1;
+// (0, 0) off the grid.
+__device__ __forceinline__ int2 compat_range(const GridDev& g, const int* __restrict__ off, int n, int cx, int cy,
+                                             int cz, int dy, int dz) {
+    const int z = cz + dz, y = cy + dy;
+    if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) return make_int2(0, 0);
+    const int rb = (z * g.gy + y) * g.gx;
+    const int s = min(max(__ldg(&off[rb + max(cx - 1, 0)]), 0), n);
+    const int e = min(max(__ldg(&off[rb + min(cx + 1, g.gx - 1) + 1]), s), n);
+    return make_int2(s, e);
+}
+
+// Row (dy, dz) for this round: useA / useB select the targets, same: b shares a's rows.
+__device__ __forceinline__ CompatRow compat_row(const GridDev& g, const int* __restrict__ off, int n, bool useA,
+                                                bool useB, bool same, int cxa, int cya, int cza, int cxb, int cyb,
+                                                int czb, int dy, int dz) {
+    CompatRow r{0, 0, 0, INT_MAX};
+    if (useA) {
+        const int2 a = compat_range(g, off, n, cxa, cya, cza, dy, dz);
+        r.s = a.x;
+        r.e = a.y;
+        r.ea = a.y;
+        if (same) {
+            const int2 b = compat_range(g, off, n, cxb, cyb, czb, dy, dz);
+            r.e = max(a.y, b.y);
+            r.sb = b.x;
+        }
+    } else if (useB) {
+        const int2 b = compat_range(g, off, n, cxb, cyb, czb, dy, dz);
+        r.s = b.x;
+        r.e = b.y;
+        r.ea = INT_MIN;
+        r.sb = b.x;
+    }
+    return r;
+}
+
+// One window, all lanes of the warp in lockstep, two candidates per step.
+__device__ __forceinline__ void compat_walk(const float4* __restrict__ p, int kl, const CompatRow& R, float2 nx,
+                                            float2 ny, float2 nz, float2& pot) {
+    const int L = R.e - R.s;
+    const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
+    for (int v = 0; v < maxL; v += 2) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int w = v + u;
+            const bool ok = w < L;
+            const int j = R.s + w;
+            const float4 q = __ldg(&p[ok ? j : kl]);
+            compat2(q, ok && j < R.ea, ok && j >= R.sb, nx, ny, nz, pot);
+        }
+    }
+}
+
+// The 9 rows of this round: the own row in two windows around the targets ([s, lo_self) and
+// [hi_self, e)), then opposite rows (-y, +y), (-z, +z), (-y-z, +y+z), (+y-z, -y+z).
+__device__ __forceinline__ void compat_rows(const GridDev& g, const float4* __restrict__ p,
+                                            const int* __restrict__ off, int n, int kl, int lo_self, int hi_self,
+                                            bool useA, bool useB, bool same, int cxa, int cya, int cza, int cxb,
+                                            int cyb, int czb, float2 nx, float2 ny, float2 nz, float2& pot) {
+    {
+        const CompatRow own = compat_row(g, off, n, useA, useB, same, cxa, cya, cza, cxb, cyb, czb, 0, 0);
+        CompatRow lo = own, hi = own;
+        lo.e = max(min(own.e, lo_self), own.s);
+        hi.s = min(max(own.s, hi_self), own.e);
+        compat_walk(p, kl, lo, nx, ny, nz, pot);
+        compat_walk(p, kl, hi, nx, ny, nz, pot);
+    }
+#pragma unroll 1
+    for (int q = 0; q < 8; ++q) {
+        // (-y, +y), (-z, +z), (-y-z, +y+z), (+y-z, -y+z): each row followed by its opposite
+        const int h = q >> 1, sg = (q & 1) ? -1 : 1;
+        const int dy = sg * (h == 0 ? -1 : (h == 1 ? 0 : (h == 2 ? -1 : 1)));
+        const int dz = sg * (h == 0 ? 0 : -1);
+        compat_walk(p, kl, compat_row(g, off, n, useA, useB, same, cxa, cya, cza, cxb, cyb, czb, dy, dz), nx, ny, nz,
+                    pot);
+    }
+}
+
 __global__ void __launch_bounds__(kPairThreads) k_pair_compat(GridDev g, const float4* __restrict__ p,
                                                               const int* __restrict__ cs,
                                                               const int* __restrict__ off, int n,
                                                               float* __restrict__ v, unsigned* status) {
-    const int k = blockIdx.x * kPairThreads + threadIdx.x;
-    if (k >= n) return;
-    const float4 pi = p[k];
-    int c = cs[k];
-    if (c < 0 || c >= g.gx * g.gy * g.gz) {
-        atomicOr(status, kFlagRange);
-        c = 0;
-    }
-    int cx, cy, cz;
-    decode_cell(g, c, cx, cy, cz);
-    const int xl = max(cx - 1, 0), xh = min(cx + 1, g.gx - 1);
-    float pot = 0.f;
-    for (int z = max(cz - 1, 0); z <= min(cz + 1, g.gz - 1); ++z)
-        for (int y = max(cy - 1, 0); y <= min(cy + 1, g.gy - 1); ++y) {
-            const int rb = (z * g.gy + y) * g.gx;
-            const int s = min(max(__ldg(&off[rb + xl]), 0), n);
-            const int e = min(max(__ldg(&off[rb + xh + 1]), s), n);
-            for (int j = s; j < e; ++j) {
-                if (j == k) continue;
-                const float4 q = __ldg(&p[j]);
-                const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-                const float r = sqrtf(dx * dx + dy * dy + dz * dz + 1e-5f);
-                const float sdr = 1.0f / r;
-                const float r6 = (sdr * sdr) * (sdr * sdr) * (sdr * sdr);
-                const float r12 = r6 * r6;
-                pot += 4.0f * (r12 - r6);
-            }
+    const int ka = 2 * (blockIdx.x * kPairThreads + (int)threadIdx.x), kb = ka + 1;
+    const bool activeA = ka < n, activeB = kb < n;
+    const int ncell = g.gx * g.gy * g.gz;
+    const float far = 1e30f;  // a parked target: every squared distance overflows to +inf
+    float4 pa = make_float4(far, far, far, 0.f), pb = pa;
+    int cxa = 0, cya = 0, cza = 0, cxb = 0, cyb = 0, czb = 0;
+    if (activeA) {
+        int c = __ldg(&cs[ka]);
+        if (c < 0 || c >= ncell) {
+            atomicOr(status, kFlagRange);
+            c = 0;
         }
-    v[k] = pot;
+        decode_cell(g, c, cxa, cya, cza);
+        pa = __ldg(&p[ka]);
+    }
+    if (activeB) {
+        int c = __ldg(&cs[kb]);
+        if (c < 0 || c >= ncell) {
+            atomicOr(status, kFlagRange);
+            c = 0;
+        }
+        decode_cell(g, c, cxb, cyb, czb);
+        pb = __ldg(&p[kb]);
+    }
+    const bool same = activeA && activeB && cya == cyb && cza == czb && cxb >= cxa;
+    const bool apart = activeB && !same;
+    const int kl = min(ka, n - 1);
+    const float2 nx = make_float2(-pa.x, -pb.x), ny = make_float2(-pa.y, -pb.y), nz = make_float2(-pa.z, -pb.z);
+    float2 pot = make_float2(0.f, 0.f);
+    // round 1: a, and b when it shares a's rows (the own row walked around both)
+    compat_rows(g, p, off, n, kl, ka, same ? kb + 1 : ka + 1, activeA, false, same, cxa, cya, cza, cxb, cyb, czb, nx,
+                ny, nz, pot);
+    // round 2: b alone, only in warps holding a lane whose targets lie in different rows
+    if (__any_sync(0xffffffffu, apart))
+        compat_rows(g, p, off, n, kl, kb, kb + 1, false, apart, false, cxa, cya, cza, cxb, cyb, czb, nx, ny, nz, pot);
+    if (same) {  // the pair (a, b), left out of the own row: each counts when in the other's 3 cells
+        const bool ba = cxb <= cxa + 1;  // symmetric: cxb >= cxa in one row
+        const float4 qb = pb;
+        const float4 qa = pa;
+        float2 t = make_float2(0.f, 0.f);
+        // a's partner b in half x (the y half masked), then b's partner a in half y
+        compat2(qb, ba, false, nx, ny, nz, t);
+        compat2(qa, false, ba, nx, ny, nz, t);
+        pot = __fadd2_rn(pot, t);
+    }
+    if (activeA) v[ka] = 4.0f * pot.x;
+    if (activeB) v[kb] = 4.0f * pot.y;
 }
 
 float grid_slack(const lj_grid& g) {
@@ -174,7 +321,7 @@ extern "C" lj_status lj_compute_compat(lj_ctx* ctx, const lj_grid* g, int n, con
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
     if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
     if (n == 0) return LJ_OK;
-    k_pair_compat<<<(n + kPairThreads - 1) / kPairThreads, kPairThreads, 0, ctx->stream>>>(
+    k_pair_compat<<<(n + 2 * kPairThreads - 1) / (2 * kPairThreads), kPairThreads, 0, ctx->stream>>>(
         to_dev(*g), reinterpret_cast<const float4*>(sorted_xyzi), sorted_cell, offsets, n, v, ctx->d_status);
     return last_launch_status();
 }
