@@ -318,7 +318,7 @@ def run_ours(args, cfg):
     ctx.sync()
     t_bin = np.array([ev[k][0].elapsed_time(ev[k][1]) for k in range(K)])
     t_pair = np.array([ev[k][1].elapsed_time(ev[k][2]) for k in range(K)])
-    t_step_ms = float((t_bin + t_pair).sum()) / K
+    t_step_ms = float(np.median(t_bin + t_pair))   # median of the K timed steps
     t_max_ms = allreduce_max(t_step_ms, ws, dev)
     total_pairs = allreduce_sum(float(pairs), ws, dev)
     value = total_pairs / (t_max_ms * 1e-3)
@@ -328,20 +328,39 @@ def run_ours(args, cfg):
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     peak_tflops = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
     algo_flops = FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs
-    pair_ms = float(t_pair.mean())
+    pair_ms = float(np.median(t_pair))
     achieved = algo_flops / (pair_ms * 1e-3) / 1e12
+    useful = FLOP_INTERACTING * pairs / (pair_ms * 1e-3) / 1e12
     kname = KERNEL_NAMES[pair_kernel]
     traffic = read_traffic(kname, cfg["workload"])
 
+    # errors of the last step's outputs against an FP64 reference on a stratified target sample
+    errors = None
+    if rank == 0:
+        smp = fp64_sample(g, b.offsets, b.cell[:n], b.xyzi[:n, :3].double(), rc, p.sigma)
+        errors = error_stats(*smp, energy[:n], force[:n])
+        errors["reference"] = "FP64 (torch, on the GPU) on the same positions, every particle of the 27-cell stencil"
+        del smp
+
     # the reference law on the same particles (our compat kernel), comparable with the reference arm's pair kernel
-    compat_ms = None
+    compat = None
     if rank == 0 and ws == 1 and cfg["dist"] == "uniform":
         gc = ljcell.grid_compat(float(cfg["hi"][0]), rc) if tuple(cfg["lo"]) == (0, 0, 0) else g
         bc = ctx.bin(gc, x, y, z, order=ljcell.ORDER_INDEX)
         vc = ctx.compute_compat(gc, bc)
-        compat_ms = time_events(lambda: ctx.compute_compat(gc, bc, vc), 3)
+        cc = torch.zeros(1, dtype=torch.int64, device=dev)
+        ctx.count_candidates(gc, bc.offsets, cc)
+        compat_ms = time_events(lambda: ctx.compute_compat(gc, bc, vc), 5, flush)
         ctx.sync()
-        del bc, vc
+        ccand = int(cc.item())
+        rate = ccand / (compat_ms * 1e-3)
+        compat = {"ms": compat_ms, "kernel": "k_pair_compat", "candidate_pairs": ccand,
+                  "candidate_pairs_per_s": rate,
+                  "gflops_reference_definition": 18 * rate / 1e9,   # NbFlopsPerInteraction = 18, cudaLJ.cu:550
+                  "fp32_frac": 18 * rate / 1e12 / peak_tflops,
+                  "mufu_frac": rate / (sms * 16 * sm_mhz * 1e6),  # one reciprocal square root per candidate
+                  "mufu_peak": f"{sms} SMs x 16 MUFU results per clock x {sm_mhz:.0f} MHz"}
+        del bc, vc, cc
 
     e2e = None
     if not args.no_e2e:
@@ -368,12 +387,14 @@ def run_ours(args, cfg):
                        "pair_kernel": f"{pair_kernel} ({kname}, chosen by lj_autotune_compute)",
                        "l2": "flushed between steps (256 MiB write), flush excluded from timing",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single gpu"},
-            "stage_ms": {"bin": float(t_bin.mean()), "pair": pair_ms},
+            "stage_ms": {"bin": float(np.median(t_bin)), "pair": pair_ms, "statistic": f"median of {K} steps",
+                         "step_mean": float((t_bin + t_pair).mean())},
             "pairs_per_step": pairs, "candidate_pairs_per_step": c_ref,
             "candidate_pairs_per_s": c_ref * ws / (t_max_ms * 1e-3),
             "particles_per_s": n * ws / (t_max_ms * 1e-3),
             "roofline": {"kernel": kname, "bound": "fp32", "achieved": achieved, "peak": peak_tflops,
                          "unit": "TFLOP/s", "frac": achieved / peak_tflops, "traffic": traffic,
+                         "useful_frac": useful / peak_tflops,   # 18 flop per interacting pair only
                          "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 flop x {sm_mhz:.0f} MHz (median sampled "
                                         "SM clock; MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
                          "algorithmic_flops": algo_flops},
@@ -383,8 +404,11 @@ def run_ours(args, cfg):
         }
         if cpu:
             line["cpu_baseline"] = cpu
-        if compat_ms is not None:
-            line["reference_law_pair_kernel_ms"] = compat_ms
+        if errors:
+            line["errors_vs_fp64"] = errors
+        if compat is not None:
+            line["reference_law_pair_kernel_ms"] = compat["ms"]
+            line["reference_law_pair_kernel"] = compat
         if extras:
             line["workloads"] = extras
         print(json.dumps(line), flush=True)
@@ -393,6 +417,74 @@ def run_ours(args, cfg):
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def fp64_sample(g, offsets, cell, pos64, rc, sigma, sample=4096, eps=1.0):
+    """FP64 reference of the truncated law for a stratified sample of sorted targets (torch, on the
+    GPU): each sample target against every particle of its 27-cell stencil, pairs i != j with
+    r < rc in FP64.  pos64: (n, 3) float64 positions in sorted order (the caller's, or the ones a
+    storage format keeps).  Returns (targets, energy, force, energy scale, force scale): the scales
+    are 4 eps sum (s^12 + s^6) and 24 eps sum (2 s^12 + s^6) / r, each pair term before the
+    cancellation between its repulsive and attractive parts."""
+    import torch
+
+    n = pos64.shape[0]
+    dev = pos64.device
+    gx, gy, gz = g.dim[0], g.dim[1], g.dim[2]
+    tgt = torch.linspace(0, n - 1, min(sample, n), device=dev).round().long().unique()
+    c = cell[tgt].long()
+    cx, cy, cz = c % gx, (c // gx) % gy, c // (gx * gy)
+    starts, lens = [], []
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            z, y = cz + dz, cy + dy
+            ok = (z >= 0) & (z < gz) & (y >= 0) & (y < gy)
+            rb = (z.clamp(0, gz - 1) * gy + y.clamp(0, gy - 1)) * gx
+            s = offsets[(rb + (cx - 1).clamp(min=0))].long()
+            e = offsets[(rb + (cx + 1).clamp(max=gx - 1) + 1)].long()
+            starts.append(torch.where(ok, s, torch.zeros_like(s)))
+            lens.append(torch.where(ok, e - s, torch.zeros_like(s)))
+    starts, lens = torch.stack(starts, 1).reshape(-1), torch.stack(lens, 1).reshape(-1)
+    owner = torch.repeat_interleave(torch.arange(len(tgt), device=dev).repeat_interleave(9), lens)
+    first = torch.cumsum(lens, 0) - lens
+    j = torch.repeat_interleave(starts - first, lens) + torch.arange(int(lens.sum()), device=dev)
+    i = tgt[owner]
+    d = pos64[j] - pos64[i]
+    r2 = (d * d).sum(1)
+    keep = (j != i) & (r2 < float(rc) ** 2)
+    d, r2, own = d[keep], r2[keep], owner[keep]
+    s2 = float(sigma) ** 2 / r2
+    s6 = s2 ** 3
+    s12 = s6 * s6
+    m = len(tgt)
+    e = torch.zeros(m, dtype=torch.float64, device=dev).index_add_(0, own, 4 * eps * (s12 - s6))
+    es = torch.zeros(m, dtype=torch.float64, device=dev).index_add_(0, own, 4 * eps * (s12 + s6))
+    fmag = 24 * eps * (2 * s12 - s6) / r2
+    f = torch.zeros((m, 3), dtype=torch.float64, device=dev).index_add_(0, own, -fmag[:, None] * d)
+    fs = torch.zeros(m, dtype=torch.float64, device=dev).index_add_(0, own, 24 * eps * (2 * s12 + s6) / r2.sqrt())
+    return tgt, e, f, es, fs
+
+
+def error_stats(tgt, e64, f64, es, fs, energy, force):
+    """Errors of float outputs (sorted order) against an FP64 sample: norm-wise force error, max and
+    p99 relative |F| error, max error over the force scale, relative error of the sample's total
+    energy and max energy error over its scale; particles whose FP64 results exceed the float range
+    are left out (and counted)."""
+    import torch
+
+    f = force.reshape(-1, 3)[tgt].double()
+    e = energy[tgt].double()
+    ok = (f64.abs() < 1e38).all(1) & (e64.abs() < 1e38) & (fs < 1e38) & (es < 1e38)
+    df = (f - f64)[ok].norm(dim=1)
+    fn = f64[ok].norm(dim=1)
+    rel = df[fn > 0] / fn[fn > 0]
+    q = lambda t: float(t.max()) if t.numel() else 0.0
+    return {"targets": int(len(tgt)), "excluded": int((~ok).sum()),
+            "force_normwise": float((f - f64)[ok].norm() / f64[ok].norm().clamp(min=1e-300)),
+            "force_max_rel": q(rel), "force_p99_rel": float(torch.quantile(rel, 0.99)) if rel.numel() else 0.0,
+            "force_max_over_scale": q(df[fs[ok] > 0] / fs[ok][fs[ok] > 0]),
+            "energy_sample_total_rel": float(abs(e[ok].sum() - e64[ok].sum()) / e64[ok].sum().abs().clamp(min=1e-300)),
+            "energy_max_over_scale": q((e - e64)[ok].abs()[es[ok] > 0] / es[ok][es[ok] > 0])}
 
 
 def time_events(fn, reps, flush=None):
@@ -529,12 +621,39 @@ def mixed_workload(ctx, cfg, seed, flush, reps=10):
     ctx.set_tuning(saved)
     ctx.sync()
     mixed_pairs = ljcell.totals_from_tensor(tot)["pairs"]
+    # errors of the mixed outputs against FP64 on the caller's positions and on the stored positions
+    # (FP32 x; y, z = origin + (cell + binary16 offset) * width), and of the plain outputs
+    caller = b.xyzi[:n, :3].double()
+    c = b.cell[:n].long()
+    gx, gy = g.dim[0], g.dim[1]
+    uyz = rec[:n, 1].contiguous().view(torch.int32)
+    uy = (uyz & 0xFFFF).to(torch.int16).view(torch.float16).double()
+    uz = ((uyz >> 16) & 0xFFFF).to(torch.int16).view(torch.float16).double()
+    w = float(g.width)
+    stored = torch.stack([rec[:n, 0].double(), g.origin[1] + (((c // gx) % gy).double() + uy) * w,
+                          g.origin[2] + ((c // (gx * gy)).double() + uz) * w], 1)
+    ref_caller = fp64_sample(g, b.offsets, b.cell[:n], caller, rc, p.sigma)
+    ref_stored = fp64_sample(g, b.offsets, b.cell[:n], stored, rc, p.sigma)
+    err_mixed_caller = error_stats(*ref_caller, e[:n], f[:n])
+    err_mixed_stored = error_stats(*ref_stored, e[:n], f[:n])
+    ctx.set_tuning(kern)
+    ctx.compute(g, p, b, e, f, tot)
+    ctx.set_tuning(saved)
+    err_plain = error_stats(*ref_caller, e[:n], f[:n])
     out = {"workload": cfg["workload"] + ", mixed precision", "ms_pair_plain": t_plain,
            "plain_kernel": KERNEL_NAMES[kern], "ms_pack_mixed": t_pack, "ms_pack_and_pair_mixed": t_mixed,
            "mixed_kernel": {0: "k_pair_mixed_pass2", 1: "k_pair_mixed", 2: "k_pair_mixed_reg"}[mk],
            "speedup_vs_plain": t_plain / t_mixed, "pairs_plain": plain_pairs, "pairs_mixed": mixed_pairs,
-           "errors": "stated by tests/test_gpu_mixed.py::test_mixed_dense_sample (FP64 oracle on a target sample)"}
-    del soa, b, e, f, tot, rec
+           "errors_vs_fp64": {
+               "mixed_vs_caller_positions": err_mixed_caller,
+               "mixed_vs_stored_positions": err_mixed_stored,
+               "plain_vs_caller_positions": err_plain,
+               "reference": "FP64 (torch, on the GPU) on a stratified sample of targets, every particle of the "
+                            "27-cell stencil; stored positions: FP32 x, y and z rebuilt from the binary16 offsets",
+               "bound_met": "1e-5 relative force error holds against the stored positions only: binary16 offsets "
+                            "move y, z by up to 2^-12 cell widths, and r^-13 forces turn that into percent-level "
+                            "errors against the caller's positions"}}
+    del soa, b, e, f, tot, rec, caller, stored, ref_caller, ref_stored
     torch.cuda.empty_cache()
     return out
 

@@ -226,6 +226,7 @@ lj_status e2e_setup(lj_ctx* c) {
 extern "C" lj_status lj_simulate_host(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx,
                                       const float* hy, const float* hz, float* h_energy, float* h_force,
                                       int* h_index, lj_totals* h_totals) {
+    const NvtxRange nvtx_range("lj_simulate_host");
     if (!c || !g || !p || n < 0 || (n > 0 && (!hx || !hy || !hz))) return LJ_EINVAL;
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
     if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;
@@ -359,6 +360,7 @@ lj_status e2ea_setup(lj_ctx* c) {
 extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx,
                                             const float* hy, const float* hz, float* h_energy, float* h_force,
                                             int* h_index, lj_totals* h_totals) {
+    const NvtxRange nvtx_range("lj_simulate_host_async");
     if (!c || !g || !p || n < 0 || (n > 0 && (!hx || !hy || !hz))) return LJ_EINVAL;
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
     if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;

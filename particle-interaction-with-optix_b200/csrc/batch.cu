@@ -667,18 +667,21 @@ static bool batch_args_ok(lj_ctx* ctx, lj_batch* b, const float* x, const float*
 
 extern "C" lj_status lj_batch_run(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
                                   float* energy, float* force, int* index, lj_totals* totals) {
+    const NvtxRange nvtx_range("lj_batch_run");
     if (!batch_args_ok(ctx, b, x, y, z, force)) return LJ_EINVAL;
     return batch_step(ctx, b, x, y, z, energy, force, index, totals);
 }
 
 extern "C" lj_status lj_batch_run_graph(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
                                         float* energy, float* force, int* index, lj_totals* totals) {
+    const NvtxRange nvtx_range("lj_batch_run_graph");
     if (!batch_args_ok(ctx, b, x, y, z, force)) return LJ_EINVAL;
     return batch_graph(ctx, b, x, y, z, energy, force, index, totals);
 }
 
 extern "C" lj_status lj_batch_run_separate(lj_ctx* ctx, lj_batch* b, const float* x, const float* y, const float* z,
                                            float* energy, float* force, int* index, lj_totals* totals) {
+    const NvtxRange nvtx_range("lj_batch_run_separate");
     if (!batch_args_ok(ctx, b, x, y, z, force)) return LJ_EINVAL;
     return batch_separate(ctx, b, x, y, z, energy, force, index, totals);
 }

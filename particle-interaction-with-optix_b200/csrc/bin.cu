@@ -512,6 +512,7 @@ extern "C" lj_status lj_count_cells(lj_ctx* ctx, const lj_grid* g, int n, const 
 }
 
 extern "C" lj_status lj_exclusive_scan(lj_ctx* ctx, const int* counts, long long ncells, int* offsets) {
+    const NvtxRange nvtx_range("lj_exclusive_scan");
     if (!ctx || ncells < 0 || !offsets || (ncells > 0 && !counts)) return LJ_EINVAL;
     if (ncells > (long long)INT_MAX - 1) return LJ_EUNSUPPORTED;
     return launch_scan(ctx, counts, ncells, offsets);
@@ -610,6 +611,7 @@ lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const flo
 extern "C" lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x, const float* y, const float* z,
                             int stride, lj_order order, int* counts, int* offsets, lj_cell_desc* cells,
                             lj_particles* sorted, float* sorted_xyzi, int* sorted_cell) {
+    const NvtxRange nvtx_range("lj_bin");
     long long nc;
     if (!ctx || n < 0 || stride < 1 || !counts || !offsets) return LJ_EINVAL;
     if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
@@ -629,6 +631,7 @@ extern "C" lj_status lj_bin(lj_ctx* ctx, const lj_grid* g, int n, const float* x
 
 extern "C" lj_status lj_count_candidates(lj_ctx* ctx, const lj_grid* g, const int* offsets,
                                          unsigned long long* d_count) {
+    const NvtxRange nvtx_range("lj_count_candidates");
     long long nc;
     if (!ctx || !offsets || !d_count) return LJ_EINVAL;
     lj_status s = check_grid(g, &nc);
@@ -844,6 +847,7 @@ __global__ void __launch_bounds__(256) k_reorder_emit(const float4* __restrict__
 }  // namespace ljc
 
 extern "C" lj_status lj_reorder(lj_ctx* ctx, int n, float* points, float radius) {
+    const NvtxRange nvtx_range("lj_reorder");
     if (!ctx || n < 0 || (n > 0 && !points) || !(radius > 0.0f) || !(radius < 3.4e38f)) return LJ_EINVAL;
     if (reinterpret_cast<uintptr_t>(points) & 15) return LJ_EINVAL;
     if (n == 0) return LJ_OK;

@@ -2,11 +2,21 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include "ljcell.h"
 
 namespace ljc {
+
+// An NVTX range around one C-ABI call: the stages of a step show up by name on a profiler's
+// timeline (header-only NVTX 3: without a tool attached the calls do nothing).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Bits of the context's device status word (the kernels OR them in).
 enum : unsigned {

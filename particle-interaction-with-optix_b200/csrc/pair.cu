@@ -317,6 +317,7 @@ using namespace ljc;
 
 extern "C" lj_status lj_compute_compat(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi,
                                        const int* sorted_cell, const int* offsets, float* v) {
+    const NvtxRange nvtx_range("lj_compute_compat");
     if (!ctx || !g || n < 0 || (n > 0 && (!sorted_xyzi || !sorted_cell || !offsets || !v))) return LJ_EINVAL;
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
     if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
@@ -329,6 +330,7 @@ extern "C" lj_status lj_compute_compat(lj_ctx* ctx, const lj_grid* g, int n, con
 extern "C" lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* sorted_xyzi,
                                 const int* sorted_cell, const int* offsets, lj_order order, float* energy,
                                 float* force, lj_totals* totals) {
+    const NvtxRange nvtx_range("lj_compute");
     if (!ctx || !g || !p || n < 0) return LJ_EINVAL;
     if (n > 0 && (!sorted_xyzi || !sorted_cell || !offsets)) return LJ_EINVAL;
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;

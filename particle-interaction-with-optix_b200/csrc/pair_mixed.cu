@@ -697,6 +697,7 @@ using namespace ljc;
 
 extern "C" lj_status lj_pack_mixed(lj_ctx* ctx, const lj_grid* g, int n, const float* sorted_xyzi,
                                    const int* sorted_cell, float* rec) {
+    const NvtxRange nvtx_range("lj_pack_mixed");
     if (!ctx || !g || n < 0 || (n > 0 && (!sorted_xyzi || !sorted_cell || !rec))) return LJ_EINVAL;
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
     if ((reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) || (reinterpret_cast<uintptr_t>(rec) & 7)) return LJ_EINVAL;
@@ -711,6 +712,7 @@ extern "C" lj_status lj_pack_mixed(lj_ctx* ctx, const lj_grid* g, int n, const f
 extern "C" lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* rec,
                                       const int* sorted_cell, const int* offsets, float* energy, float* force,
                                       lj_totals* totals) {
+    const NvtxRange nvtx_range("lj_compute_mixed");
     if (!ctx || !g || !p || n < 0 || (n > 0 && (!rec || !sorted_cell || !offsets))) return LJ_EINVAL;
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
     if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;

@@ -78,6 +78,7 @@ using namespace ljc;
 extern "C" lj_status lj_step_verlet(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, float dt, float mass,
                                     float* xyzi, float* vel, float* force, int* sorted_cell, int* counts, int* offsets,
                                     float* energy, lj_totals* totals) {
+    const NvtxRange nvtx_range("lj_step_verlet");
     if (!ctx || !g || !p || n < 0 || !counts || !offsets) return LJ_EINVAL;
     if (n > 0 && (!xyzi || !vel || !force || !sorted_cell)) return LJ_EINVAL;
     if (!(dt > 0.0f) || !(mass > 0.0f) || !(dt < 3.4e38f) || !(mass < 3.4e38f)) return LJ_EINVAL;
