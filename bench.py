@@ -658,8 +658,43 @@ def mixed_workload(ctx, cfg, seed, flush, reps=10):
     return out
 
 
+def half_workload(ctx, cfg, seed, flush, peak_tflops, reps=5):
+    """Half-shell evaluation (lj_compute_half: each unordered pair once, reactions applied to the
+    partner, deterministic colour phases) beside the full-shell default on the same binned particles."""
+    import torch
+    import ljcell
+
+    n, rc = cfg["n"], cfg["rc"]
+    g = ljcell.grid_from_box(cfg["lo"], cfg["hi"], rc)
+    p = ljcell.params(rc)
+    soa, _ = ctx.generate_uniform(seed, n, cfg["lo"], cfg["hi"])
+    b = ctx.bin(g, soa["x"], soa["y"], soa["z"], order=ljcell.ORDER_X)
+    e, f, tot = ctx.alloc_outputs(n)
+    cand = torch.zeros(1, dtype=torch.int64, device=ctx.device)
+    ctx.count_candidates(g, b.offsets, cand)
+    saved = ctx.get_tuning()["pair_kernel"]
+    kern, _ = ctx.autotune_compute(g, p, b)
+    t_full = time_events(lambda: ctx.compute(g, p, b, e, f, tot), reps, flush)
+    pairs_full = ljcell.totals_from_tensor(tot)["pairs"]
+    ctx.set_tuning(saved)
+    t_half = time_events(lambda: ctx.compute_half(g, p, b, e, f, tot), reps, flush)
+    ctx.sync()
+    pairs_half = ljcell.totals_from_tensor(tot)["pairs"]
+    c_ref = int(cand.item())
+    ach = (FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs_half) / (t_half * 1e-3) / 1e12
+    out = {"workload": cfg["workload"] + ", half shell", "ms_pair_half": t_half, "ms_pair_full": t_full,
+           "full_kernel": KERNEL_NAMES[kern], "speedup_vs_full": t_full / t_half,
+           "pairs_half": pairs_half, "pairs_full": pairs_full, "pairs_match": pairs_half == pairs_full,
+           "fp32_frac_half": ach / peak_tflops}
+    del soa, b, e, f, tot, cand
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_extras(ctx, dev, flush, peak_tflops):
     out = {}
+    out["half_shell_c2"] = half_workload(ctx, CONFIGS["c2"], 1234, flush, peak_tflops)
+    out["half_shell_c4"] = half_workload(ctx, CONFIGS["c4"], 1234, flush, peak_tflops)
     out["mixed_c4"] = mixed_workload(ctx, CONFIGS["c4"], 1234, flush)
     out["batched_c5"] = batched_workload(ctx, flush)
     out["shell_c3"] = single_workload(ctx, CONFIGS["c3"], 1234, flush, peak_tflops)

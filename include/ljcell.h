@@ -224,6 +224,20 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
                      const int* sorted_cell, const int* offsets, lj_order order, float* energy, float* force,
                      lj_totals* totals);
 
+/* Half-shell form of lj_compute (Newton's third law; the reference evaluates every
+ * ordered pair twice, cudaLJ.cu:319-337): each unordered pair {i, j} of the
+ * 27-cell stencil is evaluated once, by the cell of i when the cell of j is in
+ * its forward half-stencil (or, in one cell, j > i), and the reaction goes to j.
+ * Deterministic without float atomics: cells in 18 colours (period 3 in x and y,
+ * 2 in z) run one colour per launch, so no two concurrent cells write one
+ * particle, and within a cell the reactions collect in a fixed order.  Same
+ * distance test and outputs as lj_compute (energy[n], force[3n], totals with
+ * E = 1/2 sum of the per-particle energies and the ordered pair count, exactly
+ * twice the unordered one); any within-cell order (no x-windows).  Scratch:
+ * 20 bytes per particle in the context.  Asynchronous on the context's stream. */
+LJ_API lj_status lj_compute_half(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* sorted_xyzi,
+                                 const int* offsets, float* energy, float* force, lj_totals* totals);
+
 /* ------------------------------------------------------------- tuning
  * Implementation choices of the context (no counterpart in the reference,
  * whose launch shape is fixed at 128 threads per particle, cudaLJ.cu:519-520).

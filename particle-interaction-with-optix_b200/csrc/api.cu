@@ -112,6 +112,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->soa);
     cudaFree(c->reorder);
     cudaFree(c->step);
+    cudaFree(c->half);
     if (c->e2ea_ready) {
         cudaStreamSynchronize(c->up_stream);
         for (int i = 0; i < 9; ++i) cudaEventDestroy(c->e2ea_ev[i]);

@@ -121,6 +121,8 @@ struct lj_ctx {
     size_t reorder_bytes;
     void* step;                  // lj_step_verlet: moved positions, half-kicked velocities, ids
     size_t step_bytes;
+    void* half;                  // lj_compute_half: raw per-particle sums and the pair counter
+    size_t half_bytes;
     // end-to-end buffers (lj_simulate_host): device buffers, a second stream for the device-to-host
     // copies and the events that order it after the pair chunks
     void* e2e;
