@@ -61,7 +61,8 @@ __global__ void __launch_bounds__(256) k_count(GridDev g, const float* __restric
 // value in one 64-bit word, so flag and value become visible together.  The
 // look-back wait is bounded: on timeout it records kFlagTimeout and goes on.
 constexpr int kScanThreads = 256;
-constexpr int kScanTile = 4096;
+constexpr int kScanTile = 8192;
+constexpr int kScanIters = kScanTile / (kScanThreads * 4);  // int4 loads per thread
 constexpr unsigned long long kStAgg = 1ULL << 62;
 constexpr unsigned long long kStPre = 2ULL << 62;
 constexpr unsigned long long kStVal = (1ULL << 62) - 1ULL;
@@ -87,12 +88,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const int* __restrict__ c
     if (tile >= ntiles) return;  // defensive: more CTAs than tiles
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long tbase = tile * kScanTile;
-    const long long wbase = tbase + warp * 512;
+    const long long wbase = tbase + warp * (kScanIters * 128);
     const bool full = vec_ok && (tbase + kScanTile <= n);
-    int v[4][4];
+    int v[kScanIters][4];
     if (full) {
 #pragma unroll
-        for (int it = 0; it < 4; ++it) {
+        for (int it = 0; it < kScanIters; ++it) {
             const int4 q = __ldg(reinterpret_cast<const int4*>(counts + wbase + it * 128 + lane * 4));
             v[it][0] = q.x;
             v[it][1] = q.y;
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const int* __restrict__ c
         }
     } else {
 #pragma unroll
-        for (int it = 0; it < 4; ++it)
+        for (int it = 0; it < kScanIters; ++it)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const long long idx = wbase + it * 128 + lane * 4 + e;
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const int* __restrict__ c
     // warp-local exclusive prefixes (sums stay below 2^31: they are particle counts)
     int carry = 0;
 #pragma unroll
-    for (int it = 0; it < 4; ++it) {
+    for (int it = 0; it < kScanIters; ++it) {
         const int a0 = v[it][0], a1 = a0 + v[it][1], a2 = a1 + v[it][2], a3 = a2 + v[it][3];
         int inc = a3;
 #pragma unroll
@@ -186,12 +187,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const int* __restrict__ c
     const int tp = (int)(s_prefix + s_warp[warp]);
     if (full) {
 #pragma unroll
-        for (int it = 0; it < 4; ++it)
+        for (int it = 0; it < kScanIters; ++it)
             *reinterpret_cast<int4*>(offsets + wbase + it * 128 + lane * 4) =
                 make_int4(tp + v[it][0], tp + v[it][1], tp + v[it][2], tp + v[it][3]);
     } else {
 #pragma unroll
-        for (int it = 0; it < 4; ++it)
+        for (int it = 0; it < kScanIters; ++it)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const long long idx = wbase + it * 128 + lane * 4 + e;
