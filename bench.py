@@ -45,7 +45,8 @@ sys.path.insert(0, os.path.join(ROOT, "particle-interaction-with-optix_b200"))
 METRIC = "LJ pairs/sec @10M particles, plain vs mixed-precision/batched at ≤1e-5 err"
 FLOP_CANDIDATE = 8
 FLOP_INTERACTING = 18
-KERNEL_NAMES = {1: "k_pair_config", 2: "k_pair_direct<false>", 3: "k_pair_direct<true>", 5: "k_pair_pass<0>",
+KERNEL_NAMES = {1: "k_pair_config", 2: "k_pair_direct<false>", 3: "k_pair_direct<true>", 4: "k_pair_tiled",
+                5: "k_pair_pass<0>",
                 6: "k_pair_pass<1>", 7: "k_pair_pass<2>", 8: "k_pair_pass2<1, false>",
                 9: "k_pair_pass2<8, false>", 10: "k_pair_pass2<8, true>"}
 # launches of the pair stage per lj_compute call (kernel 7 first copies x, y, z to SoA arrays)
@@ -78,6 +79,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--pair-kernel", type=int, default=0,
+                    help="run the headline with this lj_tuning.pair_kernel instead of the autotuner's choice (profiling)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other workloads (batched 512 systems, sphere shell, dense) reported beside the headline")
     return ap.parse_args()
@@ -291,7 +294,11 @@ def run_ours(args, cfg):
     for _ in range(max(args.warmup, 3)):
         step()
     ctx.sync()
-    pair_kernel, _ = ctx.autotune_compute(g, p, b)   # outside the timed region
+    if args.pair_kernel:
+        pair_kernel = args.pair_kernel
+        ctx.set_tuning(pair_kernel)
+    else:
+        pair_kernel, _ = ctx.autotune_compute(g, p, b)   # outside the timed region
     step()
     ctx.sync()
     ctx.count_candidates(g, b.offsets, cand)
@@ -384,7 +391,8 @@ def run_ours(args, cfg):
             "dtype": "f32", "data": "synthetic (seeded drand48, device generated)",
             "config": {"workload": cfg["workload"], "n_per_gpu": n, "cutoff": rc, "sigma": p.sigma,
                        "cells": g.ncells, "order": "x-sorted within cells", "mode": "plain fp32",
-                       "pair_kernel": f"{pair_kernel} ({kname}, chosen by lj_autotune_compute)",
+                       "pair_kernel": f"{pair_kernel} ({kname}, " + ("set by --pair-kernel)" if args.pair_kernel else
+                                                                     "chosen by lj_autotune_compute)"),
                        "l2": "flushed between steps (256 MiB write), flush excluded from timing",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single gpu"},
             "stage_ms": {"bin": float(np.median(t_bin)), "pair": pair_ms, "statistic": f"median of {K} steps",
