@@ -45,12 +45,14 @@ sys.path.insert(0, os.path.join(ROOT, "particle-interaction-with-optix_b200"))
 METRIC = "LJ pairs/sec @10M particles, plain vs mixed-precision/batched at ≤1e-5 err"
 FLOP_CANDIDATE = 8
 FLOP_INTERACTING = 18
-KERNEL_NAMES = {1: "k_pair_config", 2: "k_pair_direct<false>", 3: "k_pair_direct<true>", 4: "k_pair_tiled",
-                5: "k_pair_pass<0>",
-                6: "k_pair_pass<1>", 7: "k_pair_pass<2>", 8: "k_pair_pass2<1, false>",
-                9: "k_pair_pass2<8, false>", 10: "k_pair_pass2<8, true>"}
-# launches of the pair stage per lj_compute call (kernel 7 first copies x, y, z to SoA arrays)
-PAIR_LAUNCHES = {7: 2}
+KERNEL_NAMES = {1: "k_pair_config", 6: "k_pair_pass", 10: "k_pair_pass2"}
+RETIRED = {2: 1, 3: 1, 4: 1, 5: 6, 7: 6, 8: 10, 9: 10}   # tuning values of retired variants -> the kernel they run
+
+
+def kernel_name(k: int) -> str:
+    return KERNEL_NAMES[RETIRED.get(k, k)]
+# launches of the pair stage per lj_compute call (one for every kernel)
+PAIR_LAUNCHES = {}
 SCATTER_REGION = 56 << 20   # bytes of scattered records per binning scatter pass (the library's default)
 
 
@@ -338,7 +340,7 @@ def run_ours(args, cfg):
     pair_ms = float(np.median(t_pair))
     achieved = algo_flops / (pair_ms * 1e-3) / 1e12
     useful = FLOP_INTERACTING * pairs / (pair_ms * 1e-3) / 1e12
-    kname = KERNEL_NAMES[pair_kernel]
+    kname = kernel_name(pair_kernel)
     traffic = read_traffic(kname, cfg["workload"])
 
     # errors of the last step's outputs against an FP64 reference on a stratified target sample
@@ -545,7 +547,7 @@ def single_workload(ctx, cfg, seed, flush, peak_tflops, reps=10):
     out = {"workload": cfg["workload"], "n": n, "cells": g.ncells, "ms_per_step": step,
            "stage_ms": {"bin": t_bin, "pair": t_pair}, "pairs_per_step": pairs, "pairs_per_s": pairs / (step * 1e-3),
            "particles_per_s": n / (step * 1e-3),
-           "pair_kernel_fp32": {"kernel": KERNEL_NAMES[kern], "achieved_tflops": ach, "frac": ach / peak_tflops}}
+           "pair_kernel_fp32": {"kernel": kernel_name(kern), "achieved_tflops": ach, "frac": ach / peak_tflops}}
     if cfg["dist"] == "sphere":
         algo_bytes = 76 * n + 16 * g.ncells
         out["step_hbm"] = {"algorithmic_bytes": algo_bytes, "achieved_gbs": algo_bytes / (step * 1e-3) / 1e9,
@@ -649,7 +651,7 @@ def mixed_workload(ctx, cfg, seed, flush, reps=10):
     ctx.set_tuning(saved)
     err_plain = error_stats(*ref_caller, e[:n], f[:n])
     out = {"workload": cfg["workload"] + ", mixed precision", "ms_pair_plain": t_plain,
-           "plain_kernel": KERNEL_NAMES[kern], "ms_pack_mixed": t_pack, "ms_pack_and_pair_mixed": t_mixed,
+           "plain_kernel": kernel_name(kern), "ms_pack_mixed": t_pack, "ms_pack_and_pair_mixed": t_mixed,
            "mixed_kernel": {0: "k_pair_mixed_pass2", 1: "k_pair_mixed", 2: "k_pair_mixed_reg"}[mk],
            "speedup_vs_plain": t_plain / t_mixed, "pairs_plain": plain_pairs, "pairs_mixed": mixed_pairs,
            "errors_vs_fp64": {
@@ -691,7 +693,7 @@ def half_workload(ctx, cfg, seed, flush, peak_tflops, reps=5):
     c_ref = int(cand.item())
     ach = (FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs_half) / (t_half * 1e-3) / 1e12
     out = {"workload": cfg["workload"] + ", half shell", "ms_pair_half": t_half, "ms_pair_full": t_full,
-           "full_kernel": KERNEL_NAMES[kern], "speedup_vs_full": t_full / t_half,
+           "full_kernel": kernel_name(kern), "speedup_vs_full": t_full / t_half,
            "pairs_half": pairs_half, "pairs_full": pairs_full, "pairs_match": pairs_half == pairs_full,
            "fp32_frac_half": ach / peak_tflops}
     del soa, b, e, f, tot, cand

@@ -154,7 +154,7 @@ LJ_API lj_status lj_exclusive_scan(lj_ctx* ctx, const int* counts, long long nce
  * the device-wide synchronisation cudaMalloc/cudaFree can cause -- and so
  * cannot create an lj_ctx.  Same result as lj_exclusive_scan, computed by the
  * same kernel; its look-back scratch is a fixed array inside the library
- * (256 bytes + 8 bytes per 4096 cells, 128 KiB), which every GPU that loads
+ * (256 bytes + 8 bytes per 8192 cells, 64 KiB), which every GPU that loads
  * the library holds until the process exits.
  *   - ncells <= 67,108,864 (2^26); larger returns LJ_EUNSUPPORTED.
  *   - No cudaMalloc / cudaFree and no allocating library call.
@@ -244,25 +244,21 @@ LJ_API lj_status lj_compute_half(lj_ctx* ctx, const lj_grid* g, const lj_params*
  * Results do not depend on them except in the last bits of floating-point
  * sums.  pair_kernel, for particles binned with LJ_ORDER_X:
  *   0 = default: 10 when the grid averages 2 or more particles per cell, else 6,
- *   1 = direct: one thread per target, neighbours through L1, its windows
- *       in shared memory,
- *   2 = direct with the windows in registers,
- *   3 = direct with compaction: interacting neighbours queued per lane and
- *       the pair law evaluated only for them,
- *   4 = tiled: cell-block tiles staged in shared memory by TMA bulk copies
- *       (totals summed in tile order: not bitwise reproducible run to run),
- *   5 = row passes: the 9 stencil rows walked in 5 warp-synchronous passes
- *       (opposite rows paired), coalesced neighbour loads, no divergence,
- *   6 = row passes with two candidates per step in paired FP32 instructions,
- *   7 = as 6, neighbours read from SoA copies of x, y, z in even-aligned
- *       pairs (one 8-byte load per coordinate pair; the copy is made per call),
- *   8 = row passes with two consecutive targets per lane: their windows
- *       merged, each candidate loaded once and tested against both targets
- *       in one paired FP32 evaluation,
- *   9 = as 8 with the registers capped at 64 per thread (higher occupancy),
- *  10 = as 9 with the windows parked in shared memory during the walk.
+ *   1 = one thread per target, neighbours through L1, its windows in shared
+ *       memory (also the kernel of LJ_ORDER_INDEX),
+ *   6 = row passes: the 9 stencil rows walked in 5 warp-synchronous passes
+ *       (opposite rows paired), coalesced neighbour loads, two candidates per
+ *       step in paired FP32 instructions,
+ *  10 = row passes with two consecutive targets per lane: their windows
+ *       merged, each candidate loaded once and tested against both targets in
+ *       one paired FP32 evaluation, registers capped at 64 per thread, the
+ *       windows parked in shared memory during the walk.
+ * The values 2-5 and 7-9 named variants that never won on any benchmark
+ * workload (per-lane queues, register windows, cell-block tiles staged by TMA
+ * bulk copies, scalar passes, SoA pairs); they are kept as aliases of the kernel
+ * of their family: 2, 3, 4 run 1; 5, 7 run 6; 8, 9 run 10.
  * With a non-finite coordinate (reported as LJ_ERANGE) the outputs of the
- * particles whose windows hold it are unspecified under 5-10. */
+ * particles whose windows hold it are unspecified under 6 and 10. */
 typedef struct {
     int pair_kernel;
     int scatter_passes; /* binning scatter in this many passes over cell ranges (0 = one pass per
@@ -271,7 +267,7 @@ typedef struct {
 } lj_tuning;
 
 LJ_API lj_status lj_set_tuning(lj_ctx* ctx, const lj_tuning* t);
-/* Autotuner for one system: times the deterministic pair kernels (1-3, 5-7) on
+/* Autotuner for one system: times the pair kernels 1, 6 and 10 on
  * these binned (LJ_ORDER_X) particles and keeps the fastest in the context's
  * tuning.  Synchronises. */
 LJ_API lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,
@@ -363,10 +359,10 @@ LJ_API lj_status lj_compute_mixed(lj_ctx* ctx, const lj_grid* g, const lj_params
 /* ------------------------------------------------------------- test hook
  * Failure-path check (no counterpart in the reference): runs the scan with
  * its first tile withheld, so every bounded look-back wait gives up; the next
- * lj_sync returns LJ_ETIMEOUT and the context stays usable.  ncells > 4096. */
+ * lj_sync returns LJ_ETIMEOUT and the context stays usable.  ncells > 8192. */
 LJ_API lj_status lj_test_scan_withheld_tile(lj_ctx* ctx, const int* counts, long long ncells, int* offsets);
 /* The same failure path for lj_exclusive_scan_noalloc, on its fixed array: every bounded look-back
- * wait gives up and the call marks its result invalid with offsets[ncells] = -1.  ncells > 4096. */
+ * wait gives up and the call marks its result invalid with offsets[ncells] = -1.  ncells > 8192. */
 LJ_API lj_status lj_test_scan_noalloc_withheld_tile(const int* counts, long long ncells, int* offsets, void* stream);
 
 /* ------------------------------------------------------------- time step

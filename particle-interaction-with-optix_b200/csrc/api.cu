@@ -107,9 +107,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->tmp4);
     cudaFree(c->large_cells);
     cudaFree(c->red);
-    cudaFree(c->tiles);
     cudaFree(c->e2e);
-    cudaFree(c->soa);
     cudaFree(c->reorder);
     cudaFree(c->step);
     cudaFree(c->half);
@@ -293,8 +291,7 @@ extern "C" lj_status lj_simulate_host(lj_ctx* c, const lj_grid* g, const lj_para
         cudaMemcpyAsync(h_index, didx, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, cp) != cudaSuccess)
         return LJ_ECUDA;
     // Pair stage in target chunks; chunk k's outputs go back on the copy stream during chunk k + 1.
-    // The tiled kernel (tuning 4) covers whole ranges only, so it runs as one chunk.
-    const int chunks = (c->tuning.pair_kernel == 4 || n < kE2EChunks * 4096) ? 1 : kE2EChunks;
+    const int chunks = n < kE2EChunks * 4096 ? 1 : kE2EChunks;
     for (int k = 0; k < chunks; ++k) {
         const int kb = (int)((long long)n * k / chunks), ke = (int)((long long)n * (k + 1) / chunks);
         s = launch_pair_config(c, g, p, n, dx4, dcell, doff, LJ_ORDER_X, h_energy ? de : nullptr,
@@ -434,7 +431,7 @@ extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const l
     if (n > 0 && h_index &&
         cudaMemcpyAsync(h_index, didx, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, cp) != cudaSuccess)
         return LJ_ECUDA;
-    const int chunks = (c->tuning.pair_kernel == 4 || n < kE2EChunks * 4096) ? 1 : kE2EChunks;
+    const int chunks = n < kE2EChunks * 4096 ? 1 : kE2EChunks;
     for (int k = 0; k < chunks; ++k) {
         const int kb = (int)((long long)n * k / chunks), ke = (int)((long long)n * (k + 1) / chunks);
         s = launch_pair_config(c, g, p, n, dx4, dcell, doff, LJ_ORDER_X, h_energy ? de : nullptr,

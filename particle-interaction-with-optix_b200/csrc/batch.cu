@@ -164,8 +164,7 @@ __global__ void __launch_bounds__(BLOCK) k_pair_batched(const SysDev* __restrict
                 }
             }
             PassAcc a;
-            pass_target<MODE>(S.g, S.pp, ps, nullptr, nullptr, nullptr, off + S.cell_base, S.first, S.n, k - S.first, c,
-                              active, a);
+            pass_target(S.g, S.pp, ps, off + S.cell_base, S.first, S.n, k - S.first, c, active, a);
             if (active) {
                 const float ea = a.e.x + a.e.y;
                 if (energy) energy[k] = S.pp.e4 * ea;

@@ -113,10 +113,6 @@ struct lj_ctx {
     size_t red_bytes;
     unsigned long long* d_cand;  // candidate-count accumulator
     lj_tuning tuning;            // implementation choices (lj_set_tuning)
-    void* tiles;                 // tile counter, tile count and cell-block tiles of the pair kernel
-    size_t tiles_bytes;
-    void* soa;                   // x, y, z arrays of the sorted particles for the SoA pair kernel
-    size_t soa_bytes;
     void* reorder;               // lj_reorder: key counts, offsets, sorted records and their keys
     size_t reorder_bytes;
     void* step;                  // lj_step_verlet: moved positions, half-kicked velocities, ids

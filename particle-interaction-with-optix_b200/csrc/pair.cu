@@ -277,18 +277,14 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
         int kernel = ctx->tuning.pair_kernel;
         if (kernel == 0) kernel = default_pair_kernel(n, *g);
         switch (kernel) {
-            case 4:  // cell-block tiles cover whole target ranges only; a sub-range runs kernel 1
-                if (kb == 0 && ke == n) return launch_pair_tiled(ctx, g, pp, n, xyzi, off, energy, force, totals);
-                break;
-            case 7: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 2, energy, force, totals, kb, ke);
-            case 8: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 3, energy, force, totals, kb, ke);
-            case 9: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 4, energy, force, totals, kb, ke);
-            case 10: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 5, energy, force, totals, kb, ke);
-            case 6: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 1, energy, force, totals, kb, ke);
-            case 5: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, 0, energy, force, totals, kb, ke);
-            case 3: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);
-            case 2: return launch_pair_direct(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals, kb, ke);
-            default: break;  // 1: windows in shared memory (below)
+            // retired variants run the surviving kernel of their family: 2, 3, 4 -> 1; 5, 7 -> 6; 8, 9 -> 10
+            case 5:
+            case 6:
+            case 7: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, false, energy, force, totals, kb, ke);
+            case 8:
+            case 9:
+            case 10: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);
+            default: break;  // 1 (and 2, 3, 4): windows in shared memory (below)
         }
     }
     const int blocks = (ke - kb + kPairThreads - 1) / kPairThreads;
@@ -350,8 +346,8 @@ extern "C" lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj
     int best = 1;
     float bt = 3.4e38f;
     lj_status st = LJ_OK;
-    static const int kCandidates[] = {1, 2, 3, 5, 6, 7, 8, 9, 10};
-    for (int ki = 0; ki < 9 && st == LJ_OK; ++ki) {
+    static const int kCandidates[] = {1, 6, 10};
+    for (int ki = 0; ki < 3 && st == LJ_OK; ++ki) {
         const int k = kCandidates[ki];
         ctx->tuning.pair_kernel = k;
         float ms = 3.4e38f;

@@ -1,4 +1,4 @@
-// pair_common.cuh -- pieces shared by the pair kernels (pair.cu, pair_tiled.cu).
+// pair_common.cuh -- pieces shared by the pair kernels (pair.cu, pair_pass.cu, pair_half.cu, batch.cu).
 #pragma once
 
 #include <cfloat>
@@ -238,13 +238,8 @@ __device__ __forceinline__ void pair_target(const GridDev& g, const PairParams& 
 }
 
 float grid_slack(const lj_grid& g);
-lj_status launch_pair_direct(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
-                             const int* cs, const int* off, bool compact, float* energy, float* force,
-                             lj_totals* totals, int kb, int ke);
+// Row-pass walks (pair_pass.cu): one target per lane (kernel 6) or two (kernel 10).
 lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
-                           const int* cs, const int* off, int mode, float* energy, float* force,
-                           lj_totals* totals, int kb, int ke);
-lj_status launch_pair_tiled(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
-                            const int* off, float* energy, float* force, lj_totals* totals);
-
+                           const int* cs, const int* off, bool two, float* energy, float* force, lj_totals* totals,
+                           int kb, int ke);
 }  // namespace ljc

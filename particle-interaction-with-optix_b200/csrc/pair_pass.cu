@@ -8,12 +8,8 @@ namespace {
 constexpr int kPassThreads = 128;
 }  // namespace
 
-// One thread per target of [kb, ke).  MODE as pass_target.
-template <int MODE>
+// One thread per target of [kb, ke) (pass_target).
 __global__ void __launch_bounds__(kPassThreads) k_pair_pass(GridDev g, PairParams pp, const float4* __restrict__ p,
-                                                            const float* __restrict__ sx,
-                                                            const float* __restrict__ sy,
-                                                            const float* __restrict__ sz,
                                                             const int* __restrict__ cs, const int* __restrict__ off,
                                                             int n, int kb, int ke, float* __restrict__ energy,
                                                             float* __restrict__ force, Partial* part,
@@ -29,8 +25,7 @@ __global__ void __launch_bounds__(kPassThreads) k_pair_pass(GridDev g, PairParam
         }
     }
     PassAcc a;
-    pass_target<MODE>(g, pp, p, reinterpret_cast<const float2*>(sx), reinterpret_cast<const float2*>(sy),
-                      reinterpret_cast<const float2*>(sz), off, 0, n, k, c, active, a);
+    pass_target(g, pp, p, off, 0, n, k, c, active, a);
     const float ea = a.e.x + a.e.y, wa = a.w.x + a.w.y;
     if (active) {
         if (energy) energy[k] = pp.e4 * ea;
@@ -45,10 +40,10 @@ __global__ void __launch_bounds__(kPassThreads) k_pair_pass(GridDev g, PairParam
                                 (unsigned long long)a.np, part, counter, totals);
 }
 
-// Two targets per thread (pass_target2): thread t of the launch takes targets kb + 2t and kb + 2t + 1.
-// MINB: blocks per SM the register allocation must allow; SMEM: windows parked in shared memory.
-template <int MINB, bool SMEM, int BLOCK = kPassThreads>
-__global__ void __launch_bounds__(BLOCK, MINB) k_pair_pass2(GridDev g, PairParams pp, const float4* __restrict__ p,
+// Two targets per thread (pass_target2): thread t of the launch takes targets kb + 2t and kb + 2t + 1;
+// registers capped for 8 blocks per SM, the windows parked in shared memory during the walk.
+template <int BLOCK = kPassThreads>
+__global__ void __launch_bounds__(BLOCK, 8) k_pair_pass2(GridDev g, PairParams pp, const float4* __restrict__ p,
                                                              const int* __restrict__ cs, const int* __restrict__ off,
                                                              int n, int kb, int ke, float* __restrict__ energy,
                                                              float* __restrict__ force, Partial* part,
@@ -72,12 +67,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_pass2(GridDev g, PairParam
         }
     }
     Pass2Acc a;
-    if (SMEM) {
-        __shared__ int2 s_win[9][BLOCK];
-        pass_target2<BLOCK>(g, pp, p, off, 0, n, ka, ca, cb, activeA, activeB, a, s_win);
-    } else {
-        pass_target2<BLOCK>(g, pp, p, off, 0, n, ka, ca, cb, activeA, activeB, a);
-    }
+    __shared__ int2 s_win[9][BLOCK];
+    pass_target2<BLOCK>(g, pp, p, off, 0, n, ka, ca, cb, activeA, activeB, a, s_win);
     const float nf = -pp.fscale;
     if (activeA) {
         if (energy) energy[ka] = pp.e4 * a.e.x;
@@ -100,19 +91,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_pass2(GridDev g, PairParam
                          counter, totals);
 }
 
-__global__ void __launch_bounds__(256) k_split_soa(const float4* __restrict__ p, int n, int ld, float* __restrict__ s) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + 2; i += gridDim.x * blockDim.x) {
-        const float4 q = i < n ? p[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        s[i] = q.x;
-        s[ld + i] = q.y;
-        s[2 * (size_t)ld + i] = q.z;
-    }
-}
-
 lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
-                           const int* cs, const int* off, int mode, float* energy, float* force,
-                           lj_totals* totals, int kb, int ke) {
-    const int per_block = mode >= 3 ? 2 * kPassThreads : kPassThreads;
+                           const int* cs, const int* off, bool two, float* energy, float* force, lj_totals* totals,
+                           int kb, int ke) {
+    const int per_block = two ? 2 * kPassThreads : kPassThreads;
     const int blocks = (ke - kb + per_block - 1) / per_block;
     const size_t need = 256 + (size_t)blocks * sizeof(Partial);
     if (need > ctx->red_bytes) {
@@ -124,25 +106,12 @@ lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, 
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
     const float4* p4 = reinterpret_cast<const float4*>(xyzi);
     const GridDev gd = to_dev(*g);
-    if (mode >= 3) {
-        auto kern = mode == 3 ? k_pair_pass2<1, false> : (mode == 4 ? k_pair_pass2<8, false> : k_pair_pass2<8, true>);
-        kern<<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force, part, counter,
-                                                       totals, ctx->d_status);
-    } else if (mode == 2) {
-        const int ld = (n + 2 + 63) & ~63;
-        lj_status s = grow(&ctx->soa, &ctx->soa_bytes, 3 * (size_t)ld * sizeof(float));
-        if (s != LJ_OK) return s;
-        float* sx = static_cast<float*>(ctx->soa);
-        // the SoA copy is made once per pass over all targets (the first target range starts at 0)
-        if (kb == 0) k_split_soa<<<min((n + 2 + 255) / 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(p4, n, ld, sx);
-        k_pair_pass<2><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, sx, sx + ld, sx + 2 * (size_t)ld, cs,
-                                                                 off, n, kb, ke, energy, force, part, counter,
-                                                                 totals, ctx->d_status);
-    } else {
-        auto kern = mode == 1 ? k_pair_pass<1> : k_pair_pass<0>;
-        kern<<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, nullptr, nullptr, nullptr, cs, off, n, kb, ke,
-                                                       energy, force, part, counter, totals, ctx->d_status);
-    }
+    if (two)
+        k_pair_pass2<><<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force, part,
+                                                                counter, totals, ctx->d_status);
+    else
+        k_pair_pass<<<blocks, kPassThreads, 0, ctx->stream>>>(gd, pp, p4, cs, off, n, kb, ke, energy, force, part,
+                                                              counter, totals, ctx->d_status);
     return last_launch_status();
 }
 

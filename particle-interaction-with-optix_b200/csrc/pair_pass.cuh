@@ -20,7 +20,7 @@
 // handful of cache lines instead of one line per lane, and no lane ever
 // branches away from the others: the loop bound is the warp's maximum.
 //
-// PACKED: two candidates per step evaluated with the sm_100 paired FP32
+// Two candidates per step are evaluated with the sm_100 paired FP32
 // instructions (__fadd2_rn / __fmul2_rn / __ffma2_rn), each lane of the pair
 // rounding exactly as the scalar operation.  The distance test is therefore
 // bit-identical to the scalar kernels (pair counts equal); per-target sums are
@@ -34,133 +34,53 @@
 namespace ljc {
 
 struct PassAcc {
-    float2 e, w, fx, fy, fz;  // partial sums (two for the packed form; .y unused in the scalar one)
+    float2 e, w, fx, fy, fz;  // two partial sums each (even and odd steps)
     unsigned np;
 };
 
 // One pass: window A = [sA, sA + LA), then window B = [offB + LA, offB + L).  OWN: skip j == k.
-// Packed form: a lane past the end of its windows loads record kl (a valid index: the target itself,
+// A lane past the end of its windows loads record kl (a valid index: the target itself,
 // or the last record for a lane without a target) instead of skipping the load, so no default value
 // has to be kept in registers; the masks discard it.
-template <bool PACKED, bool OWN>
+template <bool OWN>
 __device__ __forceinline__ void walk_pass(const float4* __restrict__ p, int k, int kl, const float4& pi, int sA,
                                           int LA, int offB, int L, float rc2, float sig2, PassAcc& a) {
     const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
-    if (PACKED) {
-        const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
-                     npz = make_float2(-pi.z, -pi.z);
-        const float2 nsig2 = make_float2(-sig2, -sig2), two = make_float2(2.0f, 2.0f);
-        for (int v = 0; v < maxL; v += 2) {
-            const int v1 = v + 1;
-            const bool ok0 = v < L, ok1 = v1 < L;
-            const int j0 = v + (v < LA ? sA : offB);
-            const int j1 = v1 + (v1 < LA ? sA : offB);
-            const float4 q0 = __ldg(&p[ok0 ? j0 : kl]);
-            const float4 q1 = __ldg(&p[ok1 ? j1 : kl]);
-            bool m0 = ok0, m1 = ok1;
-            if (OWN) {
-                m0 = m0 && j0 != k;
-                m1 = m1 && j1 != k;
-            }
-            const float2 dx = __fadd2_rn(make_float2(q0.x, q1.x), npx);
-            const float2 dy = __fadd2_rn(make_float2(q0.y, q1.y), npy);
-            const float2 dz = __fadd2_rn(make_float2(q0.z, q1.z), npz);
-            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-            const bool in0 = m0 && r2.x < rc2, in1 = m1 && r2.y < rc2;
-            const float2 ir2 = make_float2(rcp_hit(in0, r2.x), rcp_hit(in1, r2.y));
-            const float2 s2n = __fmul2_rn(nsig2, ir2);  // -s2
-            const float2 s4 = __fmul2_rn(s2n, s2n);     // s2 * s2
-            const float2 ns6 = __fmul2_rn(s4, s2n);     // -s6
-            const float2 s12 = __fmul2_rn(ns6, ns6);    // s6 * s6
-            a.e = __fadd2_rn(a.e, __fadd2_rn(s12, ns6));
-            const float2 t = __ffma2_rn(two, s12, ns6);  // 2 s12 - s6
-            a.w = __fadd2_rn(a.w, t);
-            const float2 fsn = __fmul2_rn(t, s2n);  // -(t s2): the sums below hold minus the force sums
-            a.fx = __ffma2_rn(fsn, dx, a.fx);
-            a.fy = __ffma2_rn(fsn, dy, a.fy);
-            a.fz = __ffma2_rn(fsn, dz, a.fz);
-            a.np += (unsigned)in0 + (unsigned)in1;
-        }
-    } else {
-        for (int v = 0; v < maxL; ++v) {
-            const bool ok = v < L;
-            const int j = v + (v < LA ? sA : offB);
-            float4 q = pi;
-            if (ok) q = __ldg(&p[j]);
-            const bool m = OWN ? (ok && j != k) : ok;
-            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            if (m && r2 < rc2) {
-                const float ir2 = rcp_approx(r2);
-                const float s2 = sig2 * ir2;
-                const float s6 = s2 * s2 * s2;
-                const float s12 = s6 * s6;
-                a.e.x += s12 - s6;
-                const float t = fmaf(2.0f, s12, -s6);
-                a.w.x += t;
-                const float fs = t * s2;
-                a.fx.x = fmaf(-fs, dx, a.fx.x);
-                a.fy.x = fmaf(-fs, dy, a.fy.x);
-                a.fz.x = fmaf(-fs, dz, a.fz.x);
-                ++a.np;
-            }
-        }
-    }
-}
-
-// Packed walk over SoA positions in aligned pairs: step t covers (j, j + 1) with j even, loaded as one
-// 8-byte load per coordinate, so each coordinate pair arrives in one register pair.  The pass's
-// windows A = [sA, eA) and B = [sB, eB) are rounded out to even starts; elements outside the window
-// (and the target itself when OWN) are masked.  x2 / y2 / z2 hold n + 1 readable elements.
-template <bool OWN>
-__device__ __forceinline__ void walk_pass_soa(const float2* __restrict__ x2, const float2* __restrict__ y2,
-                                              const float2* __restrict__ z2, int k, const float4& pi, int sA,
-                                              int eA, int sB, int eB, float rc2, float sig2, PassAcc& a) {
-    const int aA = sA & ~1, aB = sB & ~1;
-    const int PA = eA > sA ? (eA - aA + 1) >> 1 : 0;
-    const int PB = eB > sB ? (eB - aB + 1) >> 1 : 0;
-    const int P = PA + PB;
-    const int hB = (aB >> 1) - PA;  // pair index of step t in window B: hB + t
-    const int hA = aA >> 1;
-    const int maxP = (int)__reduce_max_sync(0xffffffffu, (unsigned)P);
-    const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y), npz = make_float2(-pi.z, -pi.z);
+    const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
+                 npz = make_float2(-pi.z, -pi.z);
     const float2 nsig2 = make_float2(-sig2, -sig2), two = make_float2(2.0f, 2.0f);
-    float2 qx = make_float2(pi.x, pi.x), qy = make_float2(pi.y, pi.y), qz = make_float2(pi.z, pi.z);
-    for (int t = 0; t < maxP; ++t) {
-        const bool inA = t < PA;
-        const int h = (inA ? hA : hB) + t;
-        const int j = 2 * h;
-        const int sc = inA ? sA : sB, ec = inA ? eA : eB;
-        const bool okp = t < P;
-        if (okp) {
-            qx = __ldg(&x2[h]);
-            qy = __ldg(&y2[h]);
-            qz = __ldg(&z2[h]);
-        }
-        bool m0 = okp && j >= sc, m1 = okp && j + 1 < ec;
+    for (int v = 0; v < maxL; v += 2) {
+        const int v1 = v + 1;
+        const bool ok0 = v < L, ok1 = v1 < L;
+        const int j0 = v + (v < LA ? sA : offB);
+        const int j1 = v1 + (v1 < LA ? sA : offB);
+        const float4 q0 = __ldg(&p[ok0 ? j0 : kl]);
+        const float4 q1 = __ldg(&p[ok1 ? j1 : kl]);
+        bool m0 = ok0, m1 = ok1;
         if (OWN) {
-            m0 = m0 && j != k;
-            m1 = m1 && j + 1 != k;
+            m0 = m0 && j0 != k;
+            m1 = m1 && j1 != k;
         }
-        const float2 dx = __fadd2_rn(qx, npx);
-        const float2 dy = __fadd2_rn(qy, npy);
-        const float2 dz = __fadd2_rn(qz, npz);
+        const float2 dx = __fadd2_rn(make_float2(q0.x, q1.x), npx);
+        const float2 dy = __fadd2_rn(make_float2(q0.y, q1.y), npy);
+        const float2 dz = __fadd2_rn(make_float2(q0.z, q1.z), npz);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const bool in0 = m0 && r2.x < rc2, in1 = m1 && r2.y < rc2;
         const float2 ir2 = make_float2(rcp_hit(in0, r2.x), rcp_hit(in1, r2.y));
-        const float2 s2n = __fmul2_rn(nsig2, ir2);
-        const float2 s4 = __fmul2_rn(s2n, s2n);
-        const float2 ns6 = __fmul2_rn(s4, s2n);
-        const float2 s12 = __fmul2_rn(ns6, ns6);
+        const float2 s2n = __fmul2_rn(nsig2, ir2);  // -s2
+        const float2 s4 = __fmul2_rn(s2n, s2n);     // s2 * s2
+        const float2 ns6 = __fmul2_rn(s4, s2n);     // -s6
+        const float2 s12 = __fmul2_rn(ns6, ns6);    // s6 * s6
         a.e = __fadd2_rn(a.e, __fadd2_rn(s12, ns6));
-        const float2 tt = __ffma2_rn(two, s12, ns6);
-        a.w = __fadd2_rn(a.w, tt);
-        const float2 fsn = __fmul2_rn(tt, s2n);
+        const float2 t = __ffma2_rn(two, s12, ns6);  // 2 s12 - s6
+        a.w = __fadd2_rn(a.w, t);
+        const float2 fsn = __fmul2_rn(t, s2n);  // -(t s2): the sums below hold minus the force sums
         a.fx = __ffma2_rn(fsn, dx, a.fx);
         a.fy = __ffma2_rn(fsn, dy, a.fy);
         a.fz = __ffma2_rn(fsn, dz, a.fz);
         a.np += (unsigned)in0 + (unsigned)in1;
     }
+
 }
 
 // The 9 row windows of target k (local indices in [0, n)): for row r = (dz + 1) * 3 + (dy + 1),
@@ -200,15 +120,12 @@ __device__ __forceinline__ void pass_windows(const GridDev& g, const PairParams&
     }
 }
 
-// Per-target pass walk.  Every lane of the warp must call it (inactive lanes with active = false):
-// the passes' loop bounds are warp maxima.  MODE 0: scalar, float4 neighbours; 1: packed, float4
-// neighbours; 2: packed, SoA neighbours x2 / y2 / z2 (pairs of the local arrays, even-aligned).
-// Indices k, and those of p / x2 / y2 / z2, are local: [0, n).
-template <int MODE>
+// Per-target pass walk, two candidates per step in paired FP32.  Every lane of the warp must call it
+// (inactive lanes with active = false): the passes' loop bounds are warp maxima.  Indices k, and
+// those of p, are local: [0, n).
 __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
-                                            const float2* __restrict__ x2, const float2* __restrict__ y2,
-                                            const float2* __restrict__ z2, const int* __restrict__ off, int obase,
-                                            int n, int k, int c, bool active, PassAcc& a) {
+                                            const int* __restrict__ off, int obase, int n, int k, int c, bool active,
+                                            PassAcc& a) {
     int ws[9], wl[9];
 #pragma unroll
     for (int r = 0; r < 9; ++r) ws[r] = wl[r] = 0;
@@ -220,26 +137,13 @@ __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& 
     a.e = a.w = a.fx = a.fy = a.fz = make_float2(0.f, 0.f);
     a.np = 0;
     const float rc2 = pp.rc2, sig2 = pp.sig2;
-    if (MODE == 2) {
-        walk_pass_soa<true>(x2, y2, z2, k, pi, ws[4], ws[4] + wl[4], 0, 0, rc2, sig2, a);
-        walk_pass_soa<false>(x2, y2, z2, k, pi, ws[3], ws[3] + wl[3], ws[5], ws[5] + wl[5], rc2, sig2, a);
-        walk_pass_soa<false>(x2, y2, z2, k, pi, ws[1], ws[1] + wl[1], ws[7], ws[7] + wl[7], rc2, sig2, a);
-        walk_pass_soa<false>(x2, y2, z2, k, pi, ws[0], ws[0] + wl[0], ws[8], ws[8] + wl[8], rc2, sig2, a);
-        walk_pass_soa<false>(x2, y2, z2, k, pi, ws[2], ws[2] + wl[2], ws[6], ws[6] + wl[6], rc2, sig2, a);
-    } else {
-        constexpr bool PACKED = MODE == 1;
-        const int kl = min(k, n - 1);
-        walk_pass<PACKED, true>(p, k, kl, pi, ws[4], wl[4], 0, wl[4], rc2, sig2, a);
-        walk_pass<PACKED, false>(p, k, kl, pi, ws[3], wl[3], ws[5] - wl[3], wl[3] + wl[5], rc2, sig2, a);
-        walk_pass<PACKED, false>(p, k, kl, pi, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
-        walk_pass<PACKED, false>(p, k, kl, pi, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
-        walk_pass<PACKED, false>(p, k, kl, pi, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
-    }
+    const int kl = min(k, n - 1);
+    walk_pass<true>(p, k, kl, pi, ws[4], wl[4], 0, wl[4], rc2, sig2, a);
+    walk_pass<false>(p, k, kl, pi, ws[3], wl[3], ws[5] - wl[3], wl[3] + wl[5], rc2, sig2, a);
+    walk_pass<false>(p, k, kl, pi, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
+    walk_pass<false>(p, k, kl, pi, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
+    walk_pass<false>(p, k, kl, pi, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
 }
-
-// Copies x, y, z of n sorted float4 records into three arrays (leading dimension ld >= n + 2, two
-// zero pads after the last record so the last even-aligned pair is readable).
-__global__ void k_split_soa(const float4* __restrict__ p, int n, int ld, float* __restrict__ s);
 
 }  // namespace ljc
 
@@ -365,18 +269,8 @@ __device__ __forceinline__ void pass_windows2(const GridDev& g, const PairParams
     }
 }
 
-__device__ __forceinline__ void passes2(const float4* __restrict__ p, int ka, int kb, int kl, bool useA, bool useB,
-                                        float2 nx, float2 ny, float2 nz, const int (&ws)[9], const int (&wl)[9],
-                                        float rc2, float sig2, Pass2Acc& a) {
-    walk_pass2<true>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[4], wl[4], 0, wl[4], rc2, sig2, a);
-    walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[3], wl[3], ws[5] - wl[3], wl[3] + wl[5], rc2, sig2, a);
-    walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
-    walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
-    walk_pass2<false>(p, ka, kb, kl, useA, useB, nx, ny, nz, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
-}
-
-// As passes2 with the windows read from shared memory (sw[r][threadIdx.x] = (start, length) of row r)
-// at the start of each pass, so they hold no registers during the walk.
+// The 5 passes of both targets, the windows read from shared memory (sw[r][threadIdx.x] = (start,
+// length) of row r) at the start of each pass, so they hold no registers during the walk.
 template <int BLOCK>
 __device__ __forceinline__ void passes2_smem(const float4* __restrict__ p, int ka, int kb, int kl, bool useA,
                                              bool useB, float2 nx, float2 ny, float2 nz, const int2 (*sw)[BLOCK],
@@ -398,11 +292,11 @@ __device__ __forceinline__ void passes2_smem(const float4* __restrict__ p, int k
 // Both targets of a lane (a = ka, b = ka + 1; activeA / activeB: inside the target range).  Every
 // lane of the warp must call it.  Cells ca, cb are the targets' cells (as read from the sorted cell
 // ids).  Results: a.x for target a, a.y for target b.
-// With sw (shared memory, BLOCK entries per row) the windows are parked there during the walk.
+// sw: shared memory, BLOCK entries per row, where the windows are parked during the walk.
 template <int BLOCK = 128>
 __device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams& pp, const float4* __restrict__ p,
                                              const int* __restrict__ off, int obase, int n, int ka, int ca, int cb,
-                                             bool activeA, bool activeB, Pass2Acc& a, int2 (*sw)[BLOCK] = nullptr) {
+                                             bool activeA, bool activeB, Pass2Acc& a, int2 (*sw)[BLOCK]) {
     const int kb = ka + 1;
     float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
     int ws[9], wl[9];
@@ -428,13 +322,9 @@ __device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams&
     const float rc2 = pp.rc2, sig2 = pp.sig2;
     {
         const float2 nx = make_float2(-pa.x, -pb.x), ny = make_float2(-pa.y, -pb.y), nz = make_float2(-pa.z, -pb.z);
-        if (sw) {
 #pragma unroll
-            for (int r = 0; r < 9; ++r) sw[r][threadIdx.x] = make_int2(ws[r], wl[r]);
-            passes2_smem<BLOCK>(p, ka, kb, min(ka, n - 1), activeA, same, nx, ny, nz, sw, rc2, sig2, a);
-        } else {
-            passes2(p, ka, kb, min(ka, n - 1), activeA, same, nx, ny, nz, ws, wl, rc2, sig2, a);
-        }
+        for (int r = 0; r < 9; ++r) sw[r][threadIdx.x] = make_int2(ws[r], wl[r]);
+        passes2_smem<BLOCK>(p, ka, kb, min(ka, n - 1), activeA, same, nx, ny, nz, sw, rc2, sig2, a);
     }
     if (__any_sync(0xffffffffu, straddle)) {
         if (straddle) {
@@ -444,13 +334,9 @@ __device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams&
             for (int r = 0; r < 9; ++r) ws[r] = wl[r] = 0;
         }
         const float2 nx = make_float2(-pb.x, -pb.x), ny = make_float2(-pb.y, -pb.y), nz = make_float2(-pb.z, -pb.z);
-        if (sw) {
 #pragma unroll
-            for (int r = 0; r < 9; ++r) sw[r][threadIdx.x] = make_int2(ws[r], wl[r]);
-            passes2_smem<BLOCK>(p, kb, kb, min(kb, n - 1), false, straddle, nx, ny, nz, sw, rc2, sig2, a);
-        } else {
-            passes2(p, kb, kb, min(kb, n - 1), false, straddle, nx, ny, nz, ws, wl, rc2, sig2, a);
-        }
+        for (int r = 0; r < 9; ++r) sw[r][threadIdx.x] = make_int2(ws[r], wl[r]);
+        passes2_smem<BLOCK>(p, kb, kb, min(kb, n - 1), false, straddle, nx, ny, nz, sw, rc2, sig2, a);
     }
 }
 
