@@ -224,6 +224,15 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
                      const int* sorted_cell, const int* offsets, lj_order order, float* energy, float* force,
                      lj_totals* totals);
 
+/* lj_compute for the targets [kb, ke) of the n sorted particles only (the candidates are all n):
+ * energy and force written at those indices, totals over those targets.  The piece a
+ * domain-decomposed step needs (no counterpart in the reference, which is single-GPU): a rank bins
+ * its own particles and a one-cell halo received from its neighbours, and evaluates its own
+ * particles, one contiguous sorted range when the domain is a range of z layers. */
+LJ_API lj_status lj_compute_range(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* sorted_xyzi,
+                                  const int* sorted_cell, const int* offsets, lj_order order, int kb, int ke,
+                                  float* energy, float* force, lj_totals* totals);
+
 /* Half-shell form of lj_compute (Newton's third law; the reference evaluates every
  * ordered pair twice, cudaLJ.cu:319-337): each unordered pair {i, j} of the
  * 27-cell stencil is evaluated once, by the cell of i when the cell of j is in

@@ -336,6 +336,20 @@ extern "C" lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* 
     return launch_pair_config(ctx, g, p, n, sorted_xyzi, sorted_cell, offsets, order, energy, force, totals, 0, n);
 }
 
+extern "C" lj_status lj_compute_range(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,
+                                      const float* sorted_xyzi, const int* sorted_cell, const int* offsets,
+                                      lj_order order, int kb, int ke, float* energy, float* force,
+                                      lj_totals* totals) {
+    const NvtxRange nvtx_range("lj_compute_range");
+    if (!ctx || !g || !p || n < 0 || kb < 0 || kb > ke || ke > n) return LJ_EINVAL;
+    if (n > 0 && (!sorted_xyzi || !sorted_cell || !offsets)) return LJ_EINVAL;
+    if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
+    if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;
+    if (order != LJ_ORDER_INDEX && order != LJ_ORDER_X) return LJ_EINVAL;
+    if (reinterpret_cast<uintptr_t>(sorted_xyzi) & 15) return LJ_EINVAL;
+    return launch_pair_config(ctx, g, p, n, sorted_xyzi, sorted_cell, offsets, order, energy, force, totals, kb, ke);
+}
+
 extern "C" lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,
                                          const float* sorted_xyzi, const int* sorted_cell, const int* offsets,
                                          int* best_kernel, float* best_ms) {

@@ -126,6 +126,7 @@ def _load() -> C.CDLL:
         "lj_test_scan_withheld_tile": (i32, [vp, vp, i64, vp]),
         "lj_test_scan_noalloc_withheld_tile": (i32, [vp, i64, vp, vp]),
         "lj_compute_half": (i32, [vp, vp, vp, i32, vp, vp, vp, vp, vp]),
+        "lj_compute_range": (i32, [vp, vp, vp, i32, vp, vp, vp, i32, i32, i32, vp, vp, vp]),
         "lj_reorder": (i32, [vp, i32, vp, C.c_float]),
         "lj_step_verlet": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, C.c_float, C.c_float, vp, vp, vp, vp,
                                  vp, vp, vp, vp]),
@@ -149,7 +150,7 @@ ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj
                "lj_compute_compat", "lj_compute", "lj_set_tuning", "lj_get_tuning", "lj_autotune_compute", "lj_batch_create",
                "lj_batch_destroy", "lj_batch_get_config", "lj_batch_grid", "lj_batch_run", "lj_batch_run_graph",
                "lj_batch_run_separate", "lj_batch_autotune", "lj_pack_mixed", "lj_compute_mixed",
-               "lj_test_scan_withheld_tile", "lj_test_scan_noalloc_withheld_tile", "lj_compute_half", "lj_reorder", "lj_step_verlet", "lj_simulate_host",
+               "lj_test_scan_withheld_tile", "lj_test_scan_noalloc_withheld_tile", "lj_compute_half", "lj_compute_range", "lj_reorder", "lj_step_verlet", "lj_simulate_host",
                "lj_simulate_host_async", "lj_simulate_host_wait")
 
 
@@ -263,7 +264,7 @@ class Context:
         _check(_lib.lj_set_tuning(self._h, C.byref(t)), "lj_set_tuning")
 
     def autotune_compute(self, g: Grid, p: Params, b: Binned):
-        """Times pair kernels 1-3 on these binned particles and keeps the fastest."""
+        """Times pair kernels 1, 6 and 10 on these binned particles and keeps the fastest."""
         k = C.c_int(0)
         ms = C.c_float(0)
         _check(_lib.lj_autotune_compute(self._h, C.byref(g), C.byref(p), b.n, _ptr(b.xyzi), _ptr(b.cell),
@@ -381,6 +382,15 @@ class Context:
         _check(_lib.lj_compute(self._h, C.byref(g), C.byref(p), b.n, _ptr(b.xyzi), _ptr(b.cell), _ptr(b.offsets),
                                b.order, _ptr(energy) if want_energy else None,
                                _ptr(force) if want_force else None, _ptr(totals)), "lj_compute")
+        return energy, force, totals
+
+    def compute_range(self, g: Grid, p: Params, b: Binned, kb: int, ke: int, energy=None, force=None, totals=None):
+        """lj_compute_range: the truncated law for the sorted targets [kb, ke) only."""
+        if energy is None and force is None and totals is None:
+            energy, force, totals = self.alloc_outputs(b.n)
+        _check(_lib.lj_compute_range(self._h, C.byref(g), C.byref(p), b.n, _ptr(b.xyzi), _ptr(b.cell),
+                                     _ptr(b.offsets), b.order, int(kb), int(ke), _ptr(energy), _ptr(force),
+                                     _ptr(totals)), "lj_compute_range")
         return energy, force, totals
 
     def compute_half(self, g: Grid, p: Params, b: Binned, energy=None, force=None, totals=None):
