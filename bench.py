@@ -701,8 +701,71 @@ def half_workload(ctx, cfg, seed, flush, peak_tflops, reps=5):
     return out
 
 
+def slab_workload(ctx, cfg, seed, flush, worlds=(2, 4, 8), reps=5):
+    """Slab decomposition of one system (ljcell.slab) with its W ranks emulated in turn on this
+    GPU: each rank's step (halo layers picked from its own particles, binning of own + halo on the
+    global grid, lj_compute_range over its own sorted range) timed on the device.  The exchange
+    itself is an in-memory hand-off here; the bytes a rank would receive over NVLink are reported
+    beside it.  Against the single-domain step (bin + compute) of the same system."""
+    import torch
+    import ljcell
+    from ljcell import slab
+
+    n, rc = cfg["n"], cfg["rc"]
+    g = ljcell.grid_from_box(cfg["lo"], cfg["hi"], rc)
+    p = ljcell.params(rc)
+    soa, _ = ctx.generate_uniform(seed, n, cfg["lo"], cfg["hi"])
+    xyz = torch.stack([soa["x"], soa["y"], soa["z"]], 1).contiguous()
+    del soa
+    x, y, z = (xyz[:, k].contiguous() for k in range(3))
+    b = ctx.alloc_binned(g, n, ljcell.ORDER_X)
+    e, f, tot = ctx.alloc_outputs(n)
+
+    def single():
+        ctx.bin(g, x, y, z, order=ljcell.ORDER_X, out=b)
+        ctx.compute(g, p, b, e, f, tot)
+
+    t_single = time_events(single, reps, flush)
+    ctx.sync()
+    pairs_single = ljcell.totals_from_tensor(tot)["pairs"]
+    del x, y, z, b, e, f, tot
+    torch.cuda.empty_cache()
+    out = {"workload": cfg["workload"] + ", slab ranks emulated on one GPU", "ms_single_domain": t_single,
+           "pairs_single": pairs_single, "ranks": {}}
+    for w in worlds:
+        doms = [slab.SlabDomain.of(g, r, w) for r in range(w)]
+        owns = [d.own(xyz) for d in doms]
+        halos = [d.halo_out(o) for d, o in zip(doms, owns)]
+        empty = xyz[:0]
+        ms, pairs, recv = [], 0, []
+        for r, d in enumerate(doms):
+            below = halos[r - 1][1] if r > 0 else empty
+            above = halos[r + 1][0] if r < w - 1 else empty
+            res = []
+
+            def rank_step(r=r, d=d, a=below, c=above):
+                res[:] = [slab.step(ctx, g, p, d, owns[r], exchange=lambda dom, dn, up: (a, c))]
+
+            ms.append(time_events(rank_step, reps, flush))
+            ctx.sync()
+            pairs += ljcell.totals_from_tensor(res[0].totals)["pairs"]
+            recv.append(12 * res[0].halo)
+            del res
+        out["ranks"][str(w)] = {"max_rank_ms": max(ms), "mean_rank_ms": float(np.mean(ms)),
+                                "pairs_match": pairs == pairs_single,
+                                "single_over_max_rank": t_single / max(ms),
+                                "halo_bytes_in_max": max(recv),
+                                "halo_us_at_770_gbs": max(recv) / 770e9 * 1e6}
+        del doms, owns, halos
+        torch.cuda.empty_cache()
+    del xyz
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_extras(ctx, dev, flush, peak_tflops):
     out = {}
+    out["slab_c2"] = slab_workload(ctx, CONFIGS["c2"], 1234, flush)
     out["half_shell_c2"] = half_workload(ctx, CONFIGS["c2"], 1234, flush, peak_tflops)
     out["half_shell_c4"] = half_workload(ctx, CONFIGS["c4"], 1234, flush, peak_tflops)
     out["mixed_c4"] = mixed_workload(ctx, CONFIGS["c4"], 1234, flush)
