@@ -11,10 +11,12 @@ width = cutoff (100^3 cells), eps = 1, sigma = cutoff / 2.5.
 value  = interacting ordered pairs per second over all ranks (inputs resident
          in HBM; L2 flushed between steps, flush excluded from the timing).
 e2e    = the same metric through the host-buffer entry with host buffers:
-         positions host->device, step, energy/force/index device->host, every
-         step; steps back to back through lj_simulate_host_async() (one step's
-         upload overlaps the previous step's download), the one-call
-         lj_simulate_host() time beside it.
+         positions host->device, step, energy/force device->host in the
+         caller's order, every step; steps back to back through
+         lj_simulate_host_inorder_async() (one step's upload and compute overlap
+         the previous step's download), the sorted-order entry
+         (lj_simulate_host_async, + index) and the one-call lj_simulate_host()
+         times beside it.
 roofline: the pair kernel, algorithmic flops 8 per candidate pair of the
          reference's 27-cell stencil + 18 per interacting pair, against the
          FP32 CUDA-core peak 148 SMs x 128 lanes x 2 flop x the SM clock
@@ -777,8 +779,9 @@ def run_extras(ctx, dev, flush, peak_tflops):
 
 def run_e2e(ctx, g, p, x, y, z, n, K, ws, dev, total_pairs, pairs):
     """Same metric through the host-buffer entry: pinned host positions in,
-    energy / force / index out every step, copies inside the timed region;
-    steps back to back through lj_simulate_host_async(), one
+    energy and force out every step, copies inside the timed region; steps back
+    to back through lj_simulate_host_inorder_async() (results in the caller's
+    order), with lj_simulate_host_async() (sorted order + index) and one
     lj_simulate_host() call timed beside them."""
     import torch
 
@@ -810,12 +813,27 @@ def run_e2e(ctx, g, p, x, y, z, n, K, ws, dev, total_pairs, pairs):
     t0 = time.perf_counter()
     tots = [ctx.simulate_host_async(g, p, hxn, hyn, hzn, hen, hfn, hin) for _ in range(steps)]
     ctx.simulate_host_wait()
-    e2e_s = allreduce_max((time.perf_counter() - t0) / steps, ws, dev)
+    sorted_s = allreduce_max((time.perf_counter() - t0) / steps, ws, dev)
     if any(t.pairs != pairs for t in tots):
         raise RuntimeError("pipelined end-to-end pair count differs from the device path")
+    # the same steps with energy and force returned in the caller's order (16 B per particle down, no index)
+    for _ in range(2):
+        ctx.simulate_host_inorder_async(g, p, hxn, hyn, hzn, hen, hfn)
+    ctx.simulate_host_wait()
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    tots = [ctx.simulate_host_inorder_async(g, p, hxn, hyn, hzn, hen, hfn) for _ in range(steps)]
+    ctx.simulate_host_wait()
+    e2e_s = allreduce_max((time.perf_counter() - t0) / steps, ws, dev)
+    if any(t.pairs != pairs for t in tots):
+        raise RuntimeError("input-order end-to-end pair count differs from the device path")
     return {"value": total_pairs / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": 12 * n,
-            "d2h_bytes_per_step": 20 * n + 32, "ms_per_step": e2e_s * 1e3, "steps": steps,
-            "api": "lj_simulate_host_async, steps back to back (one lj_simulate_host_wait at the end)",
+            "d2h_bytes_per_step": 16 * n + 32, "ms_per_step": e2e_s * 1e3, "steps": steps,
+            "api": "lj_simulate_host_inorder_async, steps back to back (one lj_simulate_host_wait at the end): "
+                   "energy and force in the caller's order",
+            "ms_per_step_sorted_order": sorted_s * 1e3,
+            "sorted_order_api": "lj_simulate_host_async (sorted order + index, 20 B per particle down)",
             "ms_per_step_one_call": one_s * 1e3}
 
 

@@ -427,7 +427,7 @@ LJ_API lj_status lj_simulate_host(lj_ctx* ctx, const lj_grid* g, const lj_params
  * steps back to back (no counterpart in the reference): the call returns once
  * the work is queued, and consecutive calls overlap -- the next call's
  * positions go up on an upload stream while the previous call's results come
- * down on the copy stream (PCIe carries both directions at once).  Two device
+ * down on the copy stream (PCIe carries both directions at once).  Three device
  * buffer sets in the context are used in turn.  Host buffers must be pinned
  * for the copies to overlap; the caller must leave the input buffers unchanged,
  * keep every output buffer and h_totals valid, and not read them until
@@ -440,6 +440,23 @@ LJ_API lj_status lj_simulate_host_async(lj_ctx* ctx, const lj_grid* g, const lj_
                                         int* h_index, lj_totals* h_totals);
 /* Waits for every lj_simulate_host_async call queued so far, then as lj_sync. */
 LJ_API lj_status lj_simulate_host_wait(lj_ctx* ctx);
+
+/* The same step with energy[n] and force[3n] returned in the caller's input
+ * order (particle i's results at index i), so no index array comes back: 16 B
+ * per particle down instead of 20.  The pair stage runs whole, the results are
+ * put back in input order on the device (k_unsort) and copied down while the
+ * next queued step uploads and computes.  Queued like lj_simulate_host_async
+ * (same buffer rules, completed by lj_simulate_host_wait); the two kinds of
+ * call may be mixed in one queue.  Per-particle results carry the same bits as
+ * lj_simulate_host's, permuted by its index. */
+LJ_API lj_status lj_simulate_host_inorder_async(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,
+                                                const float* hx, const float* hy, const float* hz, float* h_energy,
+                                                float* h_force, lj_totals* h_totals);
+/* lj_simulate_host_inorder_async followed by lj_simulate_host_wait (which also
+ * completes any step queued before it). */
+LJ_API lj_status lj_simulate_host_inorder(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* hx,
+                                          const float* hy, const float* hz, float* h_energy, float* h_force,
+                                          lj_totals* h_totals);
 
 #ifdef __cplusplus
 }

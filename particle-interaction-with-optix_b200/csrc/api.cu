@@ -113,7 +113,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->half);
     if (c->e2ea_ready) {
         cudaStreamSynchronize(c->up_stream);
-        for (int i = 0; i < 9; ++i) cudaEventDestroy(c->e2ea_ev[i]);
+        for (int i = 0; i < kE2EASlots + 7; ++i) cudaEventDestroy(c->e2ea_ev[i]);
         cudaStreamDestroy(c->up_stream);
     }
     if (c->e2ea_tot) {
@@ -125,8 +125,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
         for (int i = 0; i < 8; ++i) cudaEventDestroy(c->e2e_ev[i]);
         cudaStreamDestroy(c->copy_stream);
     }
-    cudaFree(c->e2ea[0]);
-    cudaFree(c->e2ea[1]);
+    for (int i = 0; i < kE2EASlots; ++i) cudaFree(c->e2ea[i]);
     delete c;
     return LJ_OK;
 }
@@ -332,15 +331,15 @@ void e2ea_deliver(lj_ctx* c) {
 lj_status e2ea_setup(lj_ctx* c) {
     if (c->e2ea_ready) return LJ_OK;
     if (cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking) != cudaSuccess) return LJ_ECUDA;
-    for (int i = 0; i < 9; ++i)
+    for (int i = 0; i < kE2EASlots + 7; ++i)
         if (cudaEventCreateWithFlags(&c->e2ea_ev[i], cudaEventDisableTiming) != cudaSuccess) {
             for (int j = 0; j < i; ++j) cudaEventDestroy(c->e2ea_ev[j]);
             cudaStreamDestroy(c->up_stream);
             c->up_stream = nullptr;
             return LJ_ECUDA;
         }
-    // both slots start free
-    for (int i = 0; i < 2; ++i)
+    // every slot starts free
+    for (int i = 0; i < kE2EASlots; ++i)
         if (cudaEventRecord(c->e2ea_ev[i], c->up_stream) != cudaSuccess) return LJ_ECUDA;
     // totals come back into pinned memory (a copy into pageable memory would make the call wait for
     // the whole step); lj_simulate_host_wait hands them to the caller
@@ -355,10 +354,33 @@ lj_status e2ea_setup(lj_ctx* c) {
 
 }  // namespace ljc
 
-extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx,
-                                            const float* hy, const float* hz, float* h_energy, float* h_force,
-                                            int* h_index, lj_totals* h_totals) {
-    const NvtxRange nvtx_range("lj_simulate_host_async");
+namespace ljc {
+
+// Results of sorted position k to the caller's order: particle idx[k] of the input.
+__global__ void k_unsort(int n, const int* __restrict__ idx, const float* __restrict__ e,
+                         const float* __restrict__ f, float* __restrict__ eo, float* __restrict__ fo,
+                         unsigned* status) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = __ldg(&idx[k]);
+        if (i < 0 || i >= n) {
+            atomicOr(status, kFlagRange);
+            continue;
+        }
+        if (eo) eo[i] = __ldg(&e[k]);
+        if (fo) {
+            fo[3 * (size_t)i + 0] = __ldg(&f[3 * (size_t)k + 0]);
+            fo[3 * (size_t)i + 1] = __ldg(&f[3 * (size_t)k + 1]);
+            fo[3 * (size_t)i + 2] = __ldg(&f[3 * (size_t)k + 2]);
+        }
+    }
+}
+
+// One queued host-buffer step (lj_simulate_host_async and lj_simulate_host_inorder_async).
+// inorder: energy and force come back in the caller's order (no index), after the whole pair stage
+// and k_unsort; otherwise in sorted order, each target chunk's results during the next chunk.
+lj_status simulate_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx, const float* hy,
+                         const float* hz, float* h_energy, float* h_force, int* h_index, lj_totals* h_totals,
+                         bool inorder) {
     if (!c || !g || !p || n < 0 || (n > 0 && (!hx || !hy || !hz))) return LJ_EINVAL;
     if (!(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;
     if (!(p->cutoff > 0.0f) || !(p->cutoff <= g->width) || !(p->sigma > 0.0f)) return LJ_EINVAL;
@@ -390,7 +412,8 @@ extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const l
     const size_t b_f = upb(3 * N * sizeof(float));
     const size_t b_idx = upb(N * sizeof(int));
     const size_t b_tot = upb((kE2EChunks + 1) * sizeof(lj_totals));
-    const size_t need = b_pos + b_cnt + b_off + b_x4 + b_cell + b_e + b_f + b_idx + b_tot;
+    const size_t b_io = inorder ? b_e + b_f : 0;  // results in the caller's order
+    const size_t need = b_pos + b_cnt + b_off + b_x4 + b_cell + b_e + b_f + b_idx + b_tot + b_io;
     if (need > c->e2ea_bytes[slot]) {
         // a grown slot: wait for its previous download on the host before freeing it
         if (cudaEventSynchronize(ev[slot]) != cudaSuccess) return LJ_ECUDA;
@@ -414,31 +437,37 @@ extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const l
     int* didx = reinterpret_cast<int*>(base);
     base += b_idx;
     lj_totals* dtot = reinterpret_cast<lj_totals*>(base);
+    base += b_tot;
+    float* deo = inorder ? reinterpret_cast<float*>(base) : nullptr;
+    float* dfo = inorder ? reinterpret_cast<float*>(base + b_e) : nullptr;
     // upload on its own stream: it overlaps the previous call's compute and downloads
     const size_t pb = (size_t)n * sizeof(float);
     if (n > 0 && (cudaMemcpyAsync(dpos, hx, pb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
                   cudaMemcpyAsync(dpos + N, hy, pb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
                   cudaMemcpyAsync(dpos + 2 * N, hz, pb, cudaMemcpyHostToDevice, up) != cudaSuccess))
         return LJ_ECUDA;
-    if (cudaEventRecord(ev[2], up) != cudaSuccess || cudaStreamWaitEvent(st, ev[2], 0) != cudaSuccess)
+    if (cudaEventRecord(ev[kE2EASlots], up) != cudaSuccess ||
+        cudaStreamWaitEvent(st, ev[kE2EASlots], 0) != cudaSuccess)
         return LJ_ECUDA;
     lj_particles sorted{};
     sorted.index = didx;
     s = lj_bin(c, g, n, dpos, dpos + N, dpos + 2 * N, 1, LJ_ORDER_X, dcnt, doff, nullptr, &sorted, dx4, dcell);
     if (s != LJ_OK) return s;
-    if (cudaEventRecord(ev[3], st) != cudaSuccess || cudaStreamWaitEvent(cp, ev[3], 0) != cudaSuccess)
+    if (cudaEventRecord(ev[kE2EASlots + 1], st) != cudaSuccess ||
+        cudaStreamWaitEvent(cp, ev[kE2EASlots + 1], 0) != cudaSuccess)
         return LJ_ECUDA;
-    if (n > 0 && h_index &&
+    if (n > 0 && h_index && !inorder &&
         cudaMemcpyAsync(h_index, didx, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, cp) != cudaSuccess)
         return LJ_ECUDA;
-    const int chunks = n < kE2EChunks * 4096 ? 1 : kE2EChunks;
+    const int chunks = inorder || n < kE2EChunks * 4096 ? 1 : kE2EChunks;
     for (int k = 0; k < chunks; ++k) {
         const int kb = (int)((long long)n * k / chunks), ke = (int)((long long)n * (k + 1) / chunks);
         s = launch_pair_config(c, g, p, n, dx4, dcell, doff, LJ_ORDER_X, h_energy ? de : nullptr,
                                h_force ? df : nullptr, dtot + k, kb, ke);
         if (s != LJ_OK) return s;
-        if (ke == kb) continue;
-        if (cudaEventRecord(ev[4 + k], st) != cudaSuccess || cudaStreamWaitEvent(cp, ev[4 + k], 0) != cudaSuccess)
+        if (ke == kb || inorder) continue;
+        if (cudaEventRecord(ev[kE2EASlots + 2 + k], st) != cudaSuccess ||
+            cudaStreamWaitEvent(cp, ev[kE2EASlots + 2 + k], 0) != cudaSuccess)
             return LJ_ECUDA;
         const size_t cb = (size_t)(ke - kb) * sizeof(float);
         if (h_energy && cudaMemcpyAsync(h_energy + kb, de + kb, cb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
@@ -448,10 +477,23 @@ extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const l
                 cudaSuccess)
             return LJ_ECUDA;
     }
+    if (inorder && n > 0 && (h_energy || h_force)) {
+        k_unsort<<<grid_for(c, n, 256), 256, 0, st>>>(n, didx, de, df, h_energy ? deo : nullptr,
+                                                       h_force ? dfo : nullptr, c->d_status);
+        if ((s = last_launch_status()) != LJ_OK) return s;
+    }
     k_sum_totals<<<1, 1, 0, st>>>(dtot, chunks, dtot + kE2EChunks);
     if ((s = last_launch_status()) != LJ_OK) return s;
-    if (cudaEventRecord(ev[8], st) != cudaSuccess || cudaStreamWaitEvent(cp, ev[8], 0) != cudaSuccess)
+    if (cudaEventRecord(ev[kE2EASlots + 6], st) != cudaSuccess ||
+        cudaStreamWaitEvent(cp, ev[kE2EASlots + 6], 0) != cudaSuccess)
         return LJ_ECUDA;
+    if (inorder && n > 0) {
+        const size_t eb = (size_t)n * sizeof(float);
+        if (h_energy && cudaMemcpyAsync(h_energy, deo, eb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
+            return LJ_ECUDA;
+        if (h_force && cudaMemcpyAsync(h_force, dfo, 3 * eb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
+            return LJ_ECUDA;
+    }
     const int q = c->e2ea_pending;
     if (cudaMemcpyAsync(c->e2ea_tot + q, dtot + kE2EChunks, sizeof(lj_totals), cudaMemcpyDeviceToHost, cp) !=
         cudaSuccess)
@@ -460,8 +502,33 @@ extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const l
     c->e2ea_pending = q + 1;
     // the slot is free again once its downloads are done
     if (cudaEventRecord(ev[slot], cp) != cudaSuccess) return LJ_ECUDA;
-    c->e2ea_slot = slot ^ 1;
+    c->e2ea_slot = (slot + 1) % kE2EASlots;
     return LJ_OK;
+}
+
+}  // namespace ljc
+
+extern "C" lj_status lj_simulate_host_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx,
+                                            const float* hy, const float* hz, float* h_energy, float* h_force,
+                                            int* h_index, lj_totals* h_totals) {
+    const NvtxRange nvtx_range("lj_simulate_host_async");
+    return simulate_async(c, g, p, n, hx, hy, hz, h_energy, h_force, h_index, h_totals, false);
+}
+
+extern "C" lj_status lj_simulate_host_inorder_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n,
+                                                    const float* hx, const float* hy, const float* hz,
+                                                    float* h_energy, float* h_force, lj_totals* h_totals) {
+    const NvtxRange nvtx_range("lj_simulate_host_inorder_async");
+    return simulate_async(c, g, p, n, hx, hy, hz, h_energy, h_force, nullptr, h_totals, true);
+}
+
+extern "C" lj_status lj_simulate_host_inorder(lj_ctx* c, const lj_grid* g, const lj_params* p, int n,
+                                              const float* hx, const float* hy, const float* hz, float* h_energy,
+                                              float* h_force, lj_totals* h_totals) {
+    const NvtxRange nvtx_range("lj_simulate_host_inorder");
+    const lj_status s = simulate_async(c, g, p, n, hx, hy, hz, h_energy, h_force, nullptr, h_totals, true);
+    const lj_status w = c ? lj_simulate_host_wait(c) : LJ_EINVAL;
+    return s != LJ_OK ? s : w;
 }
 
 extern "C" lj_status lj_simulate_host_wait(lj_ctx* c) {

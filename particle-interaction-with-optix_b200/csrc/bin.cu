@@ -461,12 +461,6 @@ __global__ void __launch_bounds__(256) k_candidates(GridDev g, const int* __rest
 }
 
 // ---------------------------------------------------------------- host side
-static inline int grid_for(const lj_ctx* ctx, long long items, int per_block, int waves = 8) {
-    long long b = (items + per_block - 1) / per_block;
-    const long long cap = (long long)ctx->sm_count * waves;
-    if (b > cap) b = cap;
-    return (int)(b < 1 ? 1 : b);
-}
 
 static lj_status check_grid(const lj_grid* g, long long* ncells) {
     if (!g || !(g->width > 0.0f) || g->dim[0] < 1 || g->dim[1] < 1 || g->dim[2] < 1) return LJ_EINVAL;

@@ -95,6 +95,12 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 
 }  // namespace ljc
 
+// Device buffer sets of the queued host-buffer steps.  Three, so that a step's upload never waits
+// for a download: with two, the upload of step k + 1 waits for the download of step k - 1, and a
+// step whose results go down only after its whole pair stage (the input-order entry) then sets a
+// period of (upload + compute + download) / 2 instead of the slowest of the three.
+constexpr int kE2EASlots = 3;
+
 // Opaque context (host side).
 struct lj_ctx {
     int device;
@@ -126,19 +132,30 @@ struct lj_ctx {
     cudaStream_t copy_stream;
     cudaEvent_t e2e_ev[8];
     bool e2e_ready;
-    // pipelined host-buffer steps (lj_simulate_host_async): two device buffer sets used in turn, an
-    // upload stream, and events: [0..1] slot free (its last download done), [2] upload done,
-    // [3] binning done, [4..7] pair chunks done, [8] totals done
-    void* e2ea[2];
-    size_t e2ea_bytes[2];
+    // pipelined host-buffer steps (lj_simulate_host_async): kE2EASlots device buffer sets used in
+    // turn, an upload stream, and events: [0, S) slot free (its last download done), then at S + 0
+    // upload done, S + 1 binning done, S + 2 .. S + 5 pair chunks done, S + 6 totals done
+    void* e2ea[kE2EASlots];
+    size_t e2ea_bytes[kE2EASlots];
     int e2ea_slot;
     cudaStream_t up_stream;
-    cudaEvent_t e2ea_ev[9];
+    cudaEvent_t e2ea_ev[kE2EASlots + 7];
     bool e2ea_ready;
     lj_totals* e2ea_tot;         // pinned staging of the queued calls' totals (kE2EAPending entries)
     lj_totals* e2ea_dst[64];     // caller's totals pointer of each queued call
     int e2ea_pending;
 };
+
+namespace ljc {
+// Blocks for a grid-stride loop over `items`: enough for every item, at most `waves` per SM.
+inline int grid_for(const lj_ctx* ctx, long long items, int per_block, int waves = 8) {
+    long long b = (items + per_block - 1) / per_block;
+    const long long cap = (long long)ctx->sm_count * waves;
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+}  // namespace ljc
+
 
 namespace ljc {
 // Host helpers shared by the .cu files (defined in api.cu).

@@ -135,6 +135,10 @@ def _load() -> C.CDLL:
         "lj_simulate_host_async": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
                                    C.POINTER(Totals)]),
         "lj_simulate_host_wait": (i32, [vp]),
+        "lj_simulate_host_inorder_async": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp,
+                                           C.POINTER(Totals)]),
+        "lj_simulate_host_inorder": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp,
+                                     C.POINTER(Totals)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -151,7 +155,8 @@ ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj
                "lj_batch_destroy", "lj_batch_get_config", "lj_batch_grid", "lj_batch_run", "lj_batch_run_graph",
                "lj_batch_run_separate", "lj_batch_autotune", "lj_pack_mixed", "lj_compute_mixed",
                "lj_test_scan_withheld_tile", "lj_test_scan_noalloc_withheld_tile", "lj_compute_half", "lj_compute_range", "lj_reorder", "lj_step_verlet", "lj_simulate_host",
-               "lj_simulate_host_async", "lj_simulate_host_wait")
+               "lj_simulate_host_async", "lj_simulate_host_wait", "lj_simulate_host_inorder_async",
+               "lj_simulate_host_inorder")
 
 
 def lib() -> C.CDLL:
@@ -456,6 +461,33 @@ class Context:
         self._pending.append((tot, hx, hy, hz, energy, force, index))
         _check(_lib.lj_simulate_host_async(self._h, C.byref(g), C.byref(p), n, fp(hx), fp(hy), fp(hz), fp(energy),
                                            fp(force), fp(index), C.byref(tot)), "lj_simulate_host_async")
+        return tot
+
+    def simulate_host_inorder_async(self, g: Grid, p: Params, hx: np.ndarray, hy: np.ndarray, hz: np.ndarray,
+                                    energy: np.ndarray | None = None, force: np.ndarray | None = None, totals=None):
+        """lj_simulate_host_inorder_async: as simulate_host_async with energy and force in the input order
+        (no index); completed by simulate_host_wait()."""
+        n = len(hx)
+        tot = totals if totals is not None else Totals()
+        fp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        if not hasattr(self, "_pending"):
+            self._pending = []
+        self._pending.append((tot, hx, hy, hz, energy, force))
+        _check(_lib.lj_simulate_host_inorder_async(self._h, C.byref(g), C.byref(p), n, fp(hx), fp(hy), fp(hz),
+                                                   fp(energy), fp(force), C.byref(tot)),
+               "lj_simulate_host_inorder_async")
+        return tot
+
+    def simulate_host_inorder(self, g: Grid, p: Params, hx: np.ndarray, hy: np.ndarray, hz: np.ndarray,
+                              energy: np.ndarray | None = None, force: np.ndarray | None = None):
+        """lj_simulate_host_inorder: one host-buffer step, energy and force in the input order."""
+        tot = Totals()
+        fp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        try:
+            _check(_lib.lj_simulate_host_inorder(self._h, C.byref(g), C.byref(p), len(hx), fp(hx), fp(hy), fp(hz),
+                                                 fp(energy), fp(force), C.byref(tot)), "lj_simulate_host_inorder")
+        finally:
+            self._pending = []
         return tot
 
     def simulate_host_wait(self):

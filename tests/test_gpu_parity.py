@@ -422,3 +422,45 @@ def test_simulate_host_async_matches_one_call(torch_cuda, ctx):
         np.testing.assert_array_equal(hf, rf)
         np.testing.assert_array_equal(hi_, ri)
         assert t.pairs == rt.pairs and t.energy == rt.energy
+
+
+@pytest.mark.parametrize("name", ["uniform_c1", "tiny33", "outside_and_faces"])
+def test_simulate_host_inorder_matches_sorted_entry(torch_cuda, ctx, name):
+    """lj_simulate_host_inorder(_async) returns energy and force in the caller's order: the sorted-order
+    results of lj_simulate_host put back through its index, bit for bit; queued input-order and
+    sorted-order calls may share one queue."""
+    torch = torch_cuda
+    import ljcell
+
+    (x, y, z), (lo, hi), rc = case_positions(name)
+    n = len(x)
+    g = ljcell.grid_from_box(lo, hi, rc)
+    p = ljcell.params(rc)
+    se, sf, si = np.empty(n, np.float32), np.empty((n, 3), np.float32), np.empty(n, np.int32)
+    st = ctx.simulate_host(g, p, x, y, z, se, sf, si)
+    want_e, want_f = np.empty_like(se), np.empty_like(sf)
+    want_e[si], want_f[si] = se, sf
+    ie, if_ = np.empty(n, np.float32), np.empty((n, 3), np.float32)
+    it = ctx.simulate_host_inorder(g, p, x, y, z, ie, if_)
+    assert np.array_equal(ie.view(np.uint32), want_e.view(np.uint32))
+    assert np.array_equal(if_.view(np.uint32), want_f.view(np.uint32))
+    assert it.pairs == st.pairs and abs(it.energy - st.energy) <= 1e-12 * abs(st.energy) + 1e-300
+
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+
+    hp = [pinned(n, torch.float32) for _ in range(3)]
+    for h, v in zip(hp, (x, y, z)):
+        h[:] = v
+    outs = [(pinned(n, torch.float32), pinned((n, 3), torch.float32)) for _ in range(3)]
+    ae, af, ai = pinned(n, torch.float32), pinned((n, 3), torch.float32), pinned(n, torch.int32)
+    tots = [ctx.simulate_host_inorder_async(g, p, *hp, *outs[0]),
+            ctx.simulate_host_async(g, p, *hp, ae, af, ai),
+            ctx.simulate_host_inorder_async(g, p, *hp, *outs[1]),
+            ctx.simulate_host_inorder_async(g, p, *hp, *outs[2])]
+    ctx.simulate_host_wait()
+    for e, f in outs:
+        assert np.array_equal(e.view(np.uint32), want_e.view(np.uint32))
+        assert np.array_equal(f.view(np.uint32), want_f.view(np.uint32))
+    assert np.array_equal(ae, se) and np.array_equal(af, sf) and np.array_equal(ai, si)
+    assert all(t.pairs == st.pairs for t in tots)
