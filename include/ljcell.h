@@ -261,7 +261,10 @@ LJ_API lj_status lj_compute_half(lj_ctx* ctx, const lj_grid* g, const lj_params*
  *  10 = row passes with two consecutive targets per lane: their windows
  *       merged, each candidate loaded once and tested against both targets in
  *       one paired FP32 evaluation, registers capped at 64 per thread, the
- *       windows parked in shared memory during the walk.
+ *       windows parked in shared memory during the walk,
+ *  11 = as 1 with the 9 rows walked whole (no row culling, no x-window
+ *       searches): on sparse grids such as a sphere shell, where a row holds
+ *       few particles, the searches cost more than the candidates they remove.
  * The values 2-5 and 7-9 named variants that never won on any benchmark
  * workload (per-lane queues, register windows, cell-block tiles staged by TMA
  * bulk copies, scalar passes, SoA pairs); they are kept as aliases of the kernel
@@ -276,7 +279,7 @@ typedef struct {
 } lj_tuning;
 
 LJ_API lj_status lj_set_tuning(lj_ctx* ctx, const lj_tuning* t);
-/* Autotuner for one system: times the pair kernels 1, 6 and 10 on
+/* Autotuner for one system: times the pair kernels 1, 6, 10 and 11 on
  * these binned (LJ_ORDER_X) particles and keeps the fastest in the context's
  * tuning.  Synchronises. */
 LJ_API lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,
@@ -443,9 +446,9 @@ LJ_API lj_status lj_simulate_host_wait(lj_ctx* ctx);
 
 /* The same step with energy[n] and force[3n] returned in the caller's input
  * order (particle i's results at index i), so no index array comes back: 16 B
- * per particle down instead of 20.  The pair stage runs whole, the results are
- * put back in input order on the device (k_unsort) and copied down while the
- * next queued step uploads and computes.  Queued like lj_simulate_host_async
+ * per particle down instead of 20.  The pair kernel writes each particle's
+ * results at its input index; they are copied down while the next queued step
+ * uploads and computes.  Queued like lj_simulate_host_async
  * (same buffer rules, completed by lj_simulate_host_wait); the two kinds of
  * call may be mixed in one queue.  Per-particle results carry the same bits as
  * lj_simulate_host's, permuted by its index. */

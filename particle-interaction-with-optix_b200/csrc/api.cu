@@ -137,7 +137,7 @@ extern "C" lj_status lj_set_stream(lj_ctx* c, void* stream) {
 }
 
 extern "C" lj_status lj_set_tuning(lj_ctx* c, const lj_tuning* t) {
-    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 10 || t->scatter_passes < 0 || t->scatter_passes > 8)
+    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 11 || t->scatter_passes < 0 || t->scatter_passes > 8)
         return LJ_EINVAL;
     c->tuning = *t;
     return LJ_OK;
@@ -356,28 +356,10 @@ lj_status e2ea_setup(lj_ctx* c) {
 
 namespace ljc {
 
-// Results of sorted position k to the caller's order: particle idx[k] of the input.
-__global__ void k_unsort(int n, const int* __restrict__ idx, const float* __restrict__ e,
-                         const float* __restrict__ f, float* __restrict__ eo, float* __restrict__ fo,
-                         unsigned* status) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int i = __ldg(&idx[k]);
-        if (i < 0 || i >= n) {
-            atomicOr(status, kFlagRange);
-            continue;
-        }
-        if (eo) eo[i] = __ldg(&e[k]);
-        if (fo) {
-            fo[3 * (size_t)i + 0] = __ldg(&f[3 * (size_t)k + 0]);
-            fo[3 * (size_t)i + 1] = __ldg(&f[3 * (size_t)k + 1]);
-            fo[3 * (size_t)i + 2] = __ldg(&f[3 * (size_t)k + 2]);
-        }
-    }
-}
-
 // One queued host-buffer step (lj_simulate_host_async and lj_simulate_host_inorder_async).
-// inorder: energy and force come back in the caller's order (no index), after the whole pair stage
-// and k_unsort; otherwise in sorted order, each target chunk's results during the next chunk.
+// inorder: the pair kernel writes energy and force at each particle's original index (the caller's
+// order, no index array), and they come back after the whole pair stage; otherwise in sorted order,
+// each target chunk's results during the next chunk.
 lj_status simulate_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n, const float* hx, const float* hy,
                          const float* hz, float* h_energy, float* h_force, int* h_index, lj_totals* h_totals,
                          bool inorder) {
@@ -412,8 +394,7 @@ lj_status simulate_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n,
     const size_t b_f = upb(3 * N * sizeof(float));
     const size_t b_idx = upb(N * sizeof(int));
     const size_t b_tot = upb((kE2EChunks + 1) * sizeof(lj_totals));
-    const size_t b_io = inorder ? b_e + b_f : 0;  // results in the caller's order
-    const size_t need = b_pos + b_cnt + b_off + b_x4 + b_cell + b_e + b_f + b_idx + b_tot + b_io;
+    const size_t need = b_pos + b_cnt + b_off + b_x4 + b_cell + b_e + b_f + b_idx + b_tot;
     if (need > c->e2ea_bytes[slot]) {
         // a grown slot: wait for its previous download on the host before freeing it
         if (cudaEventSynchronize(ev[slot]) != cudaSuccess) return LJ_ECUDA;
@@ -437,9 +418,6 @@ lj_status simulate_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n,
     int* didx = reinterpret_cast<int*>(base);
     base += b_idx;
     lj_totals* dtot = reinterpret_cast<lj_totals*>(base);
-    base += b_tot;
-    float* deo = inorder ? reinterpret_cast<float*>(base) : nullptr;
-    float* dfo = inorder ? reinterpret_cast<float*>(base + b_e) : nullptr;
     // upload on its own stream: it overlaps the previous call's compute and downloads
     const size_t pb = (size_t)n * sizeof(float);
     if (n > 0 && (cudaMemcpyAsync(dpos, hx, pb, cudaMemcpyHostToDevice, up) != cudaSuccess ||
@@ -463,7 +441,7 @@ lj_status simulate_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n,
     for (int k = 0; k < chunks; ++k) {
         const int kb = (int)((long long)n * k / chunks), ke = (int)((long long)n * (k + 1) / chunks);
         s = launch_pair_config(c, g, p, n, dx4, dcell, doff, LJ_ORDER_X, h_energy ? de : nullptr,
-                               h_force ? df : nullptr, dtot + k, kb, ke);
+                               h_force ? df : nullptr, dtot + k, kb, ke, inorder);
         if (s != LJ_OK) return s;
         if (ke == kb || inorder) continue;
         if (cudaEventRecord(ev[kE2EASlots + 2 + k], st) != cudaSuccess ||
@@ -477,11 +455,6 @@ lj_status simulate_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n,
                 cudaSuccess)
             return LJ_ECUDA;
     }
-    if (inorder && n > 0 && (h_energy || h_force)) {
-        k_unsort<<<grid_for(c, n, 256), 256, 0, st>>>(n, didx, de, df, h_energy ? deo : nullptr,
-                                                       h_force ? dfo : nullptr, c->d_status);
-        if ((s = last_launch_status()) != LJ_OK) return s;
-    }
     k_sum_totals<<<1, 1, 0, st>>>(dtot, chunks, dtot + kE2EChunks);
     if ((s = last_launch_status()) != LJ_OK) return s;
     if (cudaEventRecord(ev[kE2EASlots + 6], st) != cudaSuccess ||
@@ -489,9 +462,9 @@ lj_status simulate_async(lj_ctx* c, const lj_grid* g, const lj_params* p, int n,
         return LJ_ECUDA;
     if (inorder && n > 0) {
         const size_t eb = (size_t)n * sizeof(float);
-        if (h_energy && cudaMemcpyAsync(h_energy, deo, eb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
+        if (h_energy && cudaMemcpyAsync(h_energy, de, eb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
             return LJ_ECUDA;
-        if (h_force && cudaMemcpyAsync(h_force, dfo, 3 * eb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
+        if (h_force && cudaMemcpyAsync(h_force, df, 3 * eb, cudaMemcpyDeviceToHost, cp) != cudaSuccess)
             return LJ_ECUDA;
     }
     const int q = c->e2ea_pending;

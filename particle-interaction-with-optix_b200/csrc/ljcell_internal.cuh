@@ -177,7 +177,8 @@ lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const flo
 // Default pair kernel (lj_tuning numbering) for n particles binned in g with LJ_ORDER_X (pair.cu).
 int default_pair_kernel(int n, const lj_grid& g);
 // Pair stage of lj_compute over the sorted targets [kb, ke) (pair.cu); totals cover those targets only.
+// by_index: each target's energy and force go to its original index instead of its sorted position.
 lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm, int n, const float* xyzi,
                              const int* cs, const int* off, lj_order order, float* energy, float* force,
-                             lj_totals* totals, int kb, int ke);
+                             lj_totals* totals, int kb, int ke, bool by_index = false);
 }  // namespace ljc

@@ -57,11 +57,12 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairPar
             c = 0;
         }
         pair_target<XWIN, kPairThreads>(g, pp, p, off, n, k, c, s_win, ea, fx, fy, fz, wa, np);
-        if (energy) energy[k] = pp.e4 * ea;
-        if (force) {
-            force[3 * (size_t)k + 0] = pp.fscale * fx;
-            force[3 * (size_t)k + 1] = pp.fscale * fy;
-            force[3 * (size_t)k + 2] = pp.fscale * fz;
+        const int o = out_slot(pp, p, k, n, status);
+        if (o >= 0 && energy) energy[o] = pp.e4 * ea;
+        if (o >= 0 && force) {
+            force[3 * (size_t)o + 0] = pp.fscale * fx;
+            force[3 * (size_t)o + 1] = pp.fscale * fy;
+            force[3 * (size_t)o + 2] = pp.fscale * fz;
         }
     }
     reduce_totals<kPairThreads>(0.5 * (double)pp.e4 * (double)ea, 0.5 * (double)pp.e24 * (double)wa,
@@ -258,7 +259,7 @@ float grid_slack(const lj_grid& g) {
 
 lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm, int n, const float* xyzi,
                              const int* cs, const int* off, lj_order order, float* energy, float* force,
-                             lj_totals* totals, int kb, int ke) {
+                             lj_totals* totals, int kb, int ke, bool by_index) {
     if (ke < 0) ke = n;
     if (kb < 0 || kb > ke || ke > n) return LJ_EINVAL;
     if (kb == ke) {
@@ -273,6 +274,7 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
     pp.e24 = 24.0f * prm->epsilon;
     pp.fscale = -pp.e24 / pp.sig2;
     pp.slack = grid_slack(*g);
+    pp.by_index = by_index ? 1 : 0;
     if (order == LJ_ORDER_X) {
         int kernel = ctx->tuning.pair_kernel;
         if (kernel == 0) kernel = default_pair_kernel(n, *g);
@@ -284,7 +286,7 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
             case 8:
             case 9:
             case 10: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);
-            default: break;  // 1 (and 2, 3, 4): windows in shared memory (below)
+            default: break;  // 1 (and 2, 3, 4): windows in shared memory; 11: whole rows (below)
         }
     }
     const int blocks = (ke - kb + kPairThreads - 1) / kPairThreads;
@@ -297,7 +299,10 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
     unsigned* counter = static_cast<unsigned*>(ctx->red);
     Partial* part = reinterpret_cast<Partial*>(static_cast<char*>(ctx->red) + 256);
     const float4* p4 = reinterpret_cast<const float4*>(xyzi);
-    if (order == LJ_ORDER_X)
+    // kernel 11 walks the 9 rows whole, without the culling and x-window searches: on sparse grids
+    // (few particles per row) the searches cost more than the candidates they remove
+    const bool xwin = order == LJ_ORDER_X && ctx->tuning.pair_kernel != 11;
+    if (xwin)
         k_pair_config<true><<<blocks, kPairThreads, 0, ctx->stream>>>(to_dev(*g), pp, p4, cs, off, n, kb, ke, energy,
                                                                       force, part, counter, totals, ctx->d_status);
     else
@@ -360,8 +365,8 @@ extern "C" lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj
     int best = 1;
     float bt = 3.4e38f;
     lj_status st = LJ_OK;
-    static const int kCandidates[] = {1, 6, 10};
-    for (int ki = 0; ki < 3 && st == LJ_OK; ++ki) {
+    static const int kCandidates[] = {1, 6, 10, 11};
+    for (int ki = 0; ki < 4 && st == LJ_OK; ++ki) {
         const int k = kCandidates[ki];
         ctx->tuning.pair_kernel = k;
         float ms = 3.4e38f;

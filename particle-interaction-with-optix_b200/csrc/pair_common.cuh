@@ -22,7 +22,21 @@ struct PairParams {
     float e24;     // 24 eps
     float fscale;  // -24 eps / sigma^2: converts the accumulated sum of t * s2 * d into a force
     float slack;   // absolute rounding slack for cell planes and window ends
+    int by_index = 0;  // 1: target k's outputs go to its original index (its record's fourth word), not k
 };
+
+// Output slot of sorted target k: k, or with pp.by_index the original index stored in its record
+// (-1, and the range flag, if that index is outside [0, n)).
+__device__ __forceinline__ int out_slot(const PairParams& pp, const float4* __restrict__ p, int k, int n,
+                                        unsigned* status) {
+    if (!pp.by_index) return k;
+    const int o = __float_as_int(__ldg(&p[k].w));
+    if (o < 0 || o >= n) {
+        atomicOr(status, kFlagRange);
+        return -1;
+    }
+    return o;
+}
 
 __device__ __forceinline__ void decode_cell(const GridDev& g, int c, int& cx, int& cy, int& cz) {
     const int gxy = g.gx * g.gy;

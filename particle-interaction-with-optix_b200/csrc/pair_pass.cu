@@ -27,13 +27,14 @@ __global__ void __launch_bounds__(kPassThreads) k_pair_pass(GridDev g, PairParam
     PassAcc a;
     pass_target(g, pp, p, off, 0, n, k, c, active, a);
     const float ea = a.e.x + a.e.y, wa = a.w.x + a.w.y;
-    if (active) {
-        if (energy) energy[k] = pp.e4 * ea;
+    const int o = active ? out_slot(pp, p, k, n, status) : -1;
+    if (o >= 0) {
+        if (energy) energy[o] = pp.e4 * ea;
         if (force) {
             const float nf = -pp.fscale;
-            force[3 * (size_t)k + 0] = nf * (a.fx.x + a.fx.y);
-            force[3 * (size_t)k + 1] = nf * (a.fy.x + a.fy.y);
-            force[3 * (size_t)k + 2] = nf * (a.fz.x + a.fz.y);
+            force[3 * (size_t)o + 0] = nf * (a.fx.x + a.fx.y);
+            force[3 * (size_t)o + 1] = nf * (a.fy.x + a.fy.y);
+            force[3 * (size_t)o + 2] = nf * (a.fz.x + a.fz.y);
         }
     }
     reduce_totals<kPassThreads>(0.5 * (double)pp.e4 * (double)ea, 0.5 * (double)pp.e24 * (double)wa,
@@ -70,20 +71,22 @@ __global__ void __launch_bounds__(BLOCK, 8) k_pair_pass2(GridDev g, PairParams p
     __shared__ int2 s_win[9][BLOCK];
     pass_target2<BLOCK>(g, pp, p, off, 0, n, ka, ca, cb, activeA, activeB, a, s_win);
     const float nf = -pp.fscale;
-    if (activeA) {
-        if (energy) energy[ka] = pp.e4 * a.e.x;
+    const int oa = activeA ? out_slot(pp, p, ka, n, status) : -1;
+    const int ob = activeB ? out_slot(pp, p, ka + 1, n, status) : -1;
+    if (oa >= 0) {
+        if (energy) energy[oa] = pp.e4 * a.e.x;
         if (force) {
-            force[3 * (size_t)ka + 0] = nf * a.fx.x;
-            force[3 * (size_t)ka + 1] = nf * a.fy.x;
-            force[3 * (size_t)ka + 2] = nf * a.fz.x;
+            force[3 * (size_t)oa + 0] = nf * a.fx.x;
+            force[3 * (size_t)oa + 1] = nf * a.fy.x;
+            force[3 * (size_t)oa + 2] = nf * a.fz.x;
         }
     }
-    if (activeB) {
-        if (energy) energy[ka + 1] = pp.e4 * a.e.y;
+    if (ob >= 0) {
+        if (energy) energy[ob] = pp.e4 * a.e.y;
         if (force) {
-            force[3 * (size_t)ka + 3] = nf * a.fx.y;
-            force[3 * (size_t)ka + 4] = nf * a.fy.y;
-            force[3 * (size_t)ka + 5] = nf * a.fz.y;
+            force[3 * (size_t)ob + 0] = nf * a.fx.y;
+            force[3 * (size_t)ob + 1] = nf * a.fy.y;
+            force[3 * (size_t)ob + 2] = nf * a.fz.y;
         }
     }
     reduce_totals<BLOCK>(0.5 * (double)pp.e4 * ((double)a.e.x + (double)a.e.y),

@@ -57,8 +57,9 @@ class Particles(C.Structure):
 
 
 class Tuning(C.Structure):
-    """lj_tuning: implementation choices (pair_kernel 0 default, 1 direct with shared-memory windows,
-    2 direct with register windows, 3 direct with compaction, 4 tiled)."""
+    """lj_tuning: implementation choices (pair_kernel 0 default, 1 one target per thread with windows in
+    shared memory, 6 row passes, 10 row passes with two targets per lane, 11 as 1 with whole rows; the
+    retired values 2-5 and 7-9 run the kernel of their family)."""
 
     _fields_ = [("pair_kernel", C.c_int), ("scatter_passes", C.c_int), ("reserved", C.c_int * 6)]
 
@@ -269,7 +270,7 @@ class Context:
         _check(_lib.lj_set_tuning(self._h, C.byref(t)), "lj_set_tuning")
 
     def autotune_compute(self, g: Grid, p: Params, b: Binned):
-        """Times pair kernels 1, 6 and 10 on these binned particles and keeps the fastest."""
+        """Times pair kernels 1, 6, 10 and 11 on these binned particles and keeps the fastest."""
         k = C.c_int(0)
         ms = C.c_float(0)
         _check(_lib.lj_autotune_compute(self._h, C.byref(g), C.byref(p), b.n, _ptr(b.xyzi), _ptr(b.cell),
