@@ -34,7 +34,7 @@
 namespace ljc {
 
 struct PassAcc {
-    float2 e, w, fx, fy, fz;  // two partial sums each (even and odd steps)
+    float2 e, w, fx, fy, fz;  // two partial sums each (even and odd steps); e, w as in Pass2Acc
     unsigned np;
 };
 
@@ -71,9 +71,9 @@ __device__ __forceinline__ void walk_pass(const float4* __restrict__ p, int k, i
         const float2 s4 = __fmul2_rn(s2n, s2n);     // s2 * s2
         const float2 ns6 = __fmul2_rn(s4, s2n);     // -s6
         const float2 s12 = __fmul2_rn(ns6, ns6);    // s6 * s6
-        a.e = __fadd2_rn(a.e, __fadd2_rn(s12, ns6));
+        a.e = __fadd2_rn(a.e, s12);                  // sum s12 (converted in pass_target)
+        a.w = __fadd2_rn(a.w, ns6);                  // sum -s6
         const float2 t = __ffma2_rn(two, s12, ns6);  // 2 s12 - s6
-        a.w = __fadd2_rn(a.w, t);
         const float2 fsn = __fmul2_rn(t, s2n);  // -(t s2): the sums below hold minus the force sums
         a.fx = __ffma2_rn(fsn, dx, a.fx);
         a.fy = __ffma2_rn(fsn, dy, a.fy);
@@ -143,6 +143,9 @@ __device__ __forceinline__ void pass_target(const GridDev& g, const PairParams& 
     walk_pass<false>(p, k, kl, pi, ws[1], wl[1], ws[7] - wl[1], wl[1] + wl[7], rc2, sig2, a);
     walk_pass<false>(p, k, kl, pi, ws[0], wl[0], ws[8] - wl[0], wl[0] + wl[8], rc2, sig2, a);
     walk_pass<false>(p, k, kl, pi, ws[2], wl[2], ws[6] - wl[2], wl[2] + wl[6], rc2, sig2, a);
+    const float2 s12 = a.e, ns6 = a.w;
+    a.e = __fadd2_rn(s12, ns6);
+    a.w = __ffma2_rn(make_float2(2.0f, 2.0f), s12, ns6);
 }
 
 }  // namespace ljc
@@ -159,6 +162,10 @@ namespace ljc {
 // walks.  A lane whose targets lie in different rows walks a's windows with b masked; b's own windows
 // are walked afterwards in a second round of passes that only warps holding such a lane take.
 
+// During the walk e holds the sum of s^12 and w the sum of -s^6; pass_target2 turns them into the
+// energy sum s^12 - s^6 and the virial sum 2 s^12 - s^6 at the end, which saves one paired add per
+// candidate over summing the two combinations themselves (measured: 2.33 against 2.37 ms at 10M,
+// rc = 0.01).
 struct Pass2Acc {
     float2 e, w, fx, fy, fz;  // .x target a, .y target b
     unsigned np;
@@ -183,9 +190,9 @@ __device__ __forceinline__ void eval2(const float4& q, int j, bool ok, bool useA
     const float2 s4 = __fmul2_rn(s2n, s2n);
     const float2 ns6 = __fmul2_rn(s4, s2n);
     const float2 s12 = __fmul2_rn(ns6, ns6);
-    a.e = __fadd2_rn(a.e, __fadd2_rn(s12, ns6));
+    a.e = __fadd2_rn(a.e, s12);
+    a.w = __fadd2_rn(a.w, ns6);
     const float2 t = __ffma2_rn(make_float2(2.0f, 2.0f), s12, ns6);
-    a.w = __fadd2_rn(a.w, t);
     const float2 fsn = __fmul2_rn(t, s2n);
     a.fx = __ffma2_rn(fsn, dx, a.fx);
     a.fy = __ffma2_rn(fsn, dy, a.fy);
@@ -338,6 +345,9 @@ __device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams&
         for (int r = 0; r < 9; ++r) sw[r][threadIdx.x] = make_int2(ws[r], wl[r]);
         passes2_smem<BLOCK>(p, kb, kb, min(kb, n - 1), false, straddle, nx, ny, nz, sw, rc2, sig2, a);
     }
+    const float2 s12 = a.e, ns6 = a.w;
+    a.e = __fadd2_rn(s12, ns6);
+    a.w = __ffma2_rn(make_float2(2.0f, 2.0f), s12, ns6);
 }
 
 }  // namespace ljc
