@@ -415,6 +415,19 @@ LJ_API lj_status lj_step_verlet(lj_ctx* ctx, const lj_grid* g, const lj_params* 
  * else LJ_EUNSUPPORTED.  Scratch is the context's; asynchronous on its stream. */
 LJ_API lj_status lj_reorder(lj_ctx* ctx, int n, float* points, float radius);
 
+/* ------------------------------------------------------- slab decomposition
+ * Boundary layers of a rank's particles for the halo exchange of a spatial
+ * decomposition over z layers (no counterpart in the reference, which runs one
+ * system on one GPU).  Of the n AoS positions xyz[3n] (device), the particles
+ * whose z layer -- as lj_bin computes it for grid g -- equals layer_lo are
+ * copied, in input order, to out_lo[3 * counts[0]], and those in layer_hi to
+ * out_hi[3 * counts[1]] (device; room for n points each, or for as many as the
+ * layer can hold).  A negative layer selects nothing (its output may be NULL).
+ * counts: device int[2].  Deterministic (no atomics); three launches on the
+ * context's stream; scratch 8 bytes per 1024 particles in the context. */
+LJ_API lj_status lj_select_layers(lj_ctx* ctx, const lj_grid* g, int n, const float* xyz, int layer_lo,
+                                  int layer_hi, float* out_lo, float* out_hi, int* counts);
+
 /* ------------------------------------------------------------- end to end
  * One call with HOST buffers, the shape of executeSimulation's step
  * (cudaLJ.cu:613-653) without the generation: copies positions to the device,

@@ -111,6 +111,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->reorder);
     cudaFree(c->step);
     cudaFree(c->half);
+    cudaFree(c->sel);
     if (c->e2ea_ready) {
         cudaStreamSynchronize(c->up_stream);
         for (int i = 0; i < kE2EASlots + 7; ++i) cudaEventDestroy(c->e2ea_ev[i]);

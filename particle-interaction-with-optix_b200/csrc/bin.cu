@@ -53,8 +53,8 @@ __global__ void __launch_bounds__(256) k_count(GridDev g, const float* __restric
 
 // ---------------------------------------------------------------- scan
 // Exclusive scan of int counts[n] into offsets[0..n] (offsets[n] = total).
-// Tiles of 4096 items (256 threads x 16), tile index taken from an atomic
-// counter so every predecessor tile is already running.  Each warp scans 512
+// Tiles of 8192 items (256 threads x 32), tile index taken from an atomic
+// counter so every predecessor tile is already running.  Each warp scans 1024
 // items in a striped layout (coalesced int4 loads and stores); warp 0 then
 // publishes the tile aggregate and looks back over predecessors, 32 tiles at a
 // time, until it meets an inclusive prefix.  Tile state = 2-bit flag | 62-bit

@@ -125,6 +125,8 @@ struct lj_ctx {
     size_t step_bytes;
     void* half;                  // lj_compute_half: raw per-particle sums and the pair counter
     size_t half_bytes;
+    void* sel;                   // lj_select_layers: per-block counts, then offsets
+    size_t sel_bytes;
     // end-to-end buffers (lj_simulate_host): device buffers, a second stream for the device-to-host
     // copies and the events that order it after the pair chunks
     void* e2e;

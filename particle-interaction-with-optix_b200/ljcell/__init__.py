@@ -136,6 +136,7 @@ def _load() -> C.CDLL:
         "lj_simulate_host_async": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp, vp,
                                    C.POINTER(Totals)]),
         "lj_simulate_host_wait": (i32, [vp]),
+        "lj_select_layers": (i32, [vp, C.POINTER(Grid), i32, vp, i32, i32, vp, vp, vp]),
         "lj_simulate_host_inorder_async": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp,
                                            C.POINTER(Totals)]),
         "lj_simulate_host_inorder": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp,
@@ -157,7 +158,7 @@ ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj
                "lj_batch_run_separate", "lj_batch_autotune", "lj_pack_mixed", "lj_compute_mixed",
                "lj_test_scan_withheld_tile", "lj_test_scan_noalloc_withheld_tile", "lj_compute_half", "lj_compute_range", "lj_reorder", "lj_step_verlet", "lj_simulate_host",
                "lj_simulate_host_async", "lj_simulate_host_wait", "lj_simulate_host_inorder_async",
-               "lj_simulate_host_inorder")
+               "lj_simulate_host_inorder", "lj_select_layers")
 
 
 def lib() -> C.CDLL:
@@ -398,6 +399,21 @@ class Context:
                                      _ptr(b.offsets), b.order, int(kb), int(ke), _ptr(energy), _ptr(force),
                                      _ptr(totals)), "lj_compute_range")
         return energy, force, totals
+
+    def select_layers(self, g: Grid, xyz, layer_lo: int, layer_hi: int):
+        """lj_select_layers: the rows of the (m, 3) float32 device tensor xyz whose z layer is layer_lo,
+        and those whose z layer is layer_hi, in input order (a negative layer selects nothing).
+        Synchronises to read the two counts."""
+        t = self.torch
+        m = int(xyz.shape[0])
+        xyz = xyz.contiguous()
+        out_lo = t.empty((max(m, 1), 3), dtype=t.float32, device=self.device)
+        out_hi = t.empty((max(m, 1), 3), dtype=t.float32, device=self.device)
+        counts = t.zeros(2, dtype=t.int32, device=self.device)
+        _check(_lib.lj_select_layers(self._h, C.byref(g), m, _ptr(xyz), int(layer_lo), int(layer_hi), _ptr(out_lo),
+                                     _ptr(out_hi), _ptr(counts)), "lj_select_layers")
+        c_lo, c_hi = counts.tolist()
+        return out_lo[:c_lo], out_hi[:c_hi]
 
     def compute_half(self, g: Grid, p: Params, b: Binned, energy=None, force=None, totals=None):
         """lj_compute_half: the truncated law with each unordered pair evaluated once (any order)."""

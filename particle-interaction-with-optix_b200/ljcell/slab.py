@@ -158,16 +158,24 @@ def pair_kernel_for(dom: SlabDomain, targets: int) -> int:
 
 def step(ctx, g, p, dom: SlabDomain, own_xyz, exchange=None, order=1) -> SlabResult:
     """One decomposed evaluation on this rank (see the module docstring).  own_xyz: (m, 3) float32
-    device coordinates of the rank's own particles.  exchange(dom, down, up) -> (below, above);
+    device coordinates of the rank's own particles, all in its layers [z0, z1) (as
+    SlabDomain.own selects them).  exchange(dom, down, up) -> (below, above);
     default: exchange_p2p.  With the context's pair kernel left at 0 (default), the kernel is
-    chosen from the occupancy of the own layers; a kernel set with set_tuning is kept."""
+    chosen from the occupancy of the own layers; a kernel set with set_tuning is kept.
+
+    The boundary layers are picked on the device (lj_select_layers, input order kept); the local
+    particles [below, own, above] are binned as one AoS array.  Their sorted order puts the layer
+    below first and the layer above last (cells are ordered by z first), so the own particles are
+    the sorted positions [len(below), len(below) + m) without reading the offsets back."""
     torch = _torch()
-    down, up = dom.halo_out(own_xyz)
+    down, up = ctx.select_layers(g, own_xyz, dom.z0 if dom.rank > 0 else -1,
+                                 dom.z1 - 1 if dom.rank < dom.world - 1 else -1)
     below, above = (exchange or exchange_p2p)(dom, down, up)
     local = torch.cat([below, own_xyz, above]).contiguous()
-    x, y, z = (local[:, k].contiguous() for k in range(3))
-    b = ctx.bin(g, x, y, z, order=order)
-    kb, ke = dom.target_range(b.offsets)
+    flat = local.view(-1)
+    b = ctx.bin(g, flat, flat[1:], flat[2:], stride=3, order=order)
+    kb = int(below.shape[0])
+    ke = kb + int(own_xyz.shape[0])
     tuning = ctx.get_tuning()
     if tuning["pair_kernel"] == 0:
         ctx.set_tuning(pair_kernel_for(dom, ke - kb), tuning["scatter_passes"])

@@ -464,3 +464,28 @@ def test_simulate_host_inorder_matches_sorted_entry(torch_cuda, ctx, name):
         assert np.array_equal(f.view(np.uint32), want_f.view(np.uint32))
     assert np.array_equal(ae, se) and np.array_equal(af, sf) and np.array_equal(ai, si)
     assert all(t.pairs == st.pairs for t in tots)
+
+
+@pytest.mark.parametrize("kernel", [1, 6, 10, 11])
+def test_simulate_host_inorder_every_kernel(torch_cuda, ctx, kernel):
+    """Each pair kernel writes a target's results at its input index in the input-order entry: the
+    sorted entry's results put back through its index, bit for bit, with the same kernel."""
+    import ljcell
+
+    (x, y, z), (lo, hi), rc = case_positions("uniform_c1")
+    n = len(x)
+    g = ljcell.grid_from_box(lo, hi, rc)
+    p = ljcell.params(rc)
+    ctx.set_tuning(kernel)
+    try:
+        se, sf, si = np.empty(n, np.float32), np.empty((n, 3), np.float32), np.empty(n, np.int32)
+        st = ctx.simulate_host(g, p, x, y, z, se, sf, si)
+        ie, if_ = np.empty(n, np.float32), np.empty((n, 3), np.float32)
+        it = ctx.simulate_host_inorder(g, p, x, y, z, ie, if_)
+    finally:
+        ctx.set_tuning(0)
+    want_e, want_f = np.empty_like(se), np.empty_like(sf)
+    want_e[si], want_f[si] = se, sf
+    assert np.array_equal(ie.view(np.uint32), want_e.view(np.uint32))
+    assert np.array_equal(if_.view(np.uint32), want_f.view(np.uint32))
+    assert it.pairs == st.pairs

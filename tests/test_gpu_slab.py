@@ -57,6 +57,7 @@ def emulated_ranks(ctx, g, p, xyz, world):
         res = slab.step(ctx, g, p, d, owns[r], exchange=lambda dom, down, up, a=below, b=above: (a, b))
         local = res.binned.xyzi[res.kb:res.ke, 3].contiguous().view(torch.int32).long() - below.shape[0]
         assert res.ke - res.kb == owns[r].shape[0]
+        assert (res.kb, res.ke) == d.target_range(res.binned.offsets)
         if res.ke > res.kb:
             assert int(local.min()) >= 0 and int(local.max()) < owns[r].shape[0]
         gid = own_ids[r][local]
@@ -140,3 +141,35 @@ def test_slab_ranks_uniform_10M(torch_cuda, ctx, world):
         assert abs(h - layers * 100_000) < 5_000, (r, h)
     del xyz
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("n", [0, 1, 1023, 1024, 1025, 100_000])
+def test_select_layers_matches_host_selection(torch_cuda, ctx, n):
+    """lj_select_layers returns the particles of two z layers in input order, as the host-side
+    selection (SlabDomain.halo_out) does: same rows, same order, bit for bit; faces, points outside
+    the box and a non-finite z included; a negative layer selects nothing; both layers may be one."""
+    import ljcell
+    from ljcell import slab
+
+    torch = torch_cuda
+    rng = np.random.default_rng(n + 7)
+    xyz = rng.uniform(-0.1, 1.1, (n, 3)).astype(np.float32)
+    if n >= 8:
+        xyz[:4, 2] = np.float32(0.05) * np.arange(4, dtype=np.float32)   # on the layer faces
+        xyz[4, 2] = np.nan
+        xyz[5, 2] = np.inf
+    g = ljcell.grid_from_box((0, 0, 0), (1, 1, 1), 0.05)
+    t = torch.from_numpy(xyz).to("cuda")
+    for world, rank in ((4, 1), (4, 0), (4, 3), (20, 7)):
+        dom = slab.SlabDomain.of(g, rank, world)
+        down, up = dom.halo_out(t)
+        lo = dom.z0 if rank > 0 else -1
+        hi = dom.z1 - 1 if rank < world - 1 else -1
+        got_lo, got_hi = ctx.select_layers(g, t, lo, hi)
+        assert torch.equal(got_lo.view(torch.int32), down.view(torch.int32))
+        assert torch.equal(got_hi.view(torch.int32), up.view(torch.int32))
+    zc = slab.SlabDomain.of(g, 0, 1).z_cells(t[:, 2])
+    for layer in (0, 5, 19):
+        a, b = ctx.select_layers(g, t, layer, layer)
+        want = t[zc == layer].view(torch.int32)
+        assert torch.equal(a.view(torch.int32), want) and torch.equal(b.view(torch.int32), want)
