@@ -55,6 +55,17 @@ def full(request, ctx, torch_cuda):
     energy, force, tot = ctx.compute(g, p, b)
     ctx.sync()
     n = w["n"]
+    # the sparse-grid kernel the autotuner picks on the shell (11: whole rows)
+    extra = {}
+    if w["kind"] == "shell":
+        for k in (11,):
+            ctx.set_tuning(k)
+            try:
+                ek, fk, tk = ctx.compute(g, p, b)
+                ctx.sync()
+            finally:
+                ctx.set_tuning(0)
+            extra[k] = (np_(ek)[:n], np_(fk)[:n], ljcell.totals_from_tensor(tk))
     gpu = {
         "counts": np_(b.counts), "offsets": np_(b.offsets), "cells": np_(b.cells).reshape(-1, 2),
         "xyzi": np_(b.xyzi)[:n], "cell": np_(b.cell)[:n],
@@ -62,6 +73,7 @@ def full(request, ctx, torch_cuda):
         "index": np_(b.index)[:n],
         "candidates": int(np_(cand).reshape(-1)[0]),
         "energy": np_(energy)[:n], "force": np_(force)[:n], "totals": ljcell.totals_from_tensor(tot),
+        "extra": extra,
     }
     del d, b, cand, energy, force, tot
     torch.cuda.empty_cache()
@@ -118,6 +130,23 @@ def test_total_energy(full):
         t = gpu["totals"]
         assert abs(t["energy"] - ref.etot) <= TOTAL_ENERGY_TOL * abs(ref.etot), (t["energy"], ref.etot)
         assert abs(t["virial"] - ref.virial) <= TOTAL_ENERGY_TOL * abs(ref.virial), (t["virial"], ref.virial)
+
+
+def test_sparse_grid_kernel_on_the_shell(full):
+    """Kernel 11 (whole rows), which the autotuner picks on the shell: pair count exact, every
+    particle within tolerance, total energy within 1e-6."""
+    ref, extra = full["ref"], full["gpu"]["extra"]
+    if not extra:
+        pytest.skip("the sparse-grid kernel is run on the shell workload")
+    ok = ref.representable()
+    for k, (e, f, t) in extra.items():
+        assert t["pairs"] == ref.pairs, k
+        fe = ref.force_errors(f, FORCE_SCALED_TOL)
+        ee = ref.energy_errors(e, ENERGY_SCALED_TOL)
+        assert fe["max_scaled_over_tol"] <= 1.0 and fe["normwise"] <= FORCE_NORMWISE_TOL, (k, fe)
+        assert ee["max_scaled_over_tol"] <= 1.0, (k, ee)
+        got, want = 0.5 * e[ok].astype(np.float64).sum(), 0.5 * ref.e64[ok].sum()
+        assert abs(got - want) <= TOTAL_ENERGY_TOL * abs(want), (k, got, want)
 
 
 # ------------------------------------------------------------------ 512 uneven systems
