@@ -228,10 +228,10 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_compat(GridDev g, const f
     const int kl = min(ka, n - 1);
     const float2 nx = make_float2(-pa.x, -pb.x), ny = make_float2(-pa.y, -pb.y), nz = make_float2(-pa.z, -pb.z);
     float2 pot = make_float2(0.f, 0.f);
-    // round 1: a, and b when it shares a's rows (the own row walked around both)
+    // first sweep: a, and b when it shares a's rows (the own row walked around both)
     compat_rows(g, p, off, n, kl, ka, same ? kb + 1 : ka + 1, activeA, false, same, cxa, cya, cza, cxb, cyb, czb, nx,
                 ny, nz, pot);
-    // round 2: b alone, only in warps holding a lane whose targets lie in different rows
+    // second sweep: b alone, only in warps holding a lane whose targets lie in different rows
     if (__any_sync(0xffffffffu, apart))
         compat_rows(g, p, off, n, kl, kb, kb + 1, false, apart, false, cxa, cya, cza, cxb, cyb, czb, nx, ny, nz, pot);
     if (same) {  // the pair (a, b), left out of the own row: each counts when in the other's 3 cells
