@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_config(GridDev g, PairPar
 // and each candidate loaded once is evaluated for both targets in paired FP32, each target masked to
 // its own 3 cells and to j != itself.  The rows are taken in 5 passes, all lanes of a warp in
 // lockstep (the own row, then opposite rows paired), so the warp's loads fall on a few neighbouring
-// lines.  A lane whose targets lie in different rows walks a's rows, then, in a second round that only
+// lines.  A lane whose targets lie in different rows walks a's rows, then, in a second sweep that only
 // warps holding such a lane take, b's.
 //
 // The law is the reference's, 4 eps ((s/r)^12 - (s/r)^6) with eps = s = 1 and

@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(kMixThreads) k_pair_mixed_pass(GridDev g, MixP
 // consecutive sorted targets a = 2m and b = 2m + 1; when they share a (y, z) row of cells their
 // windows are merged and each record is loaded once and evaluated against both, the two halves of
 // every packed operand holding (j - a) and (j - b) in cell units.  A lane whose targets lie in
-// different rows walks b in a second round.  Each half rounds as k_pair_mixed, so the distance test
+// different rows walks b in a second sweep.  Each half rounds as k_pair_mixed, so the distance test
 // and the pair count are unchanged; per-target sums are compensated per pass (TwoSum), as above.
 
 struct MixAcc2 {

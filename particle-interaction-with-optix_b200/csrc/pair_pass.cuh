@@ -160,7 +160,7 @@ namespace ljc {
 // differences of (j, a) and (j, b) form the two halves of each packed operand.  Each half rounds as
 // the scalar kernels do, so the distance test and the pair count are those of the single-target
 // walks.  A lane whose targets lie in different rows walks a's windows with b masked; b's own windows
-// are walked afterwards in a second round of passes that only warps holding such a lane take.
+// are walked afterwards in a second sweep of passes that only warps holding such a lane take.
 
 // During the walk e holds the sum of s^12 and w the sum of -s^6; pass_target2 turns them into the
 // energy sum s^12 - s^6 and the virial sum 2 s^12 - s^6 at the end, which saves one paired add per
@@ -317,7 +317,7 @@ __device__ __forceinline__ void pass_target2(const GridDev& g, const PairParams&
         decode_cell(g, cb, cxb, cyb, czb);
     }
     const bool same = activeA && activeB && cya == cyb && cza == czb && cxb >= cxa;
-    const bool straddle = activeB && !same;  // b walked in the second round
+    const bool straddle = activeB && !same;  // b walked in the second sweep
     if (activeA) {
         pass_windows2(g, pp, p, off, obase, n, pa, pb, same, cxa, cxb, cya, cza, ws, wl);
     } else {
