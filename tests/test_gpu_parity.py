@@ -489,3 +489,46 @@ def test_simulate_host_inorder_every_kernel(torch_cuda, ctx, kernel):
     assert np.array_equal(ie.view(np.uint32), want_e.view(np.uint32))
     assert np.array_equal(if_.view(np.uint32), want_f.view(np.uint32))
     assert it.pairs == st.pairs
+
+
+# Grids other than the unit cube: an anisotropic box far from the origin, a single row of cells
+# (no neighbour rows in y or z), and cells twice as wide as the cutoff (a grid built for a larger
+# cutoff and reused).  box lo, hi, grid cell width, law cutoff, particles.
+GEOMETRIES = {
+    "anisotropic_offset": ((-0.3, 0.1, 2.0), (0.9, 0.35, 2.2), 0.02, 0.02, 40_000),
+    "one_row": ((0.0, 0.0, 0.0), (1.0, 0.03, 0.03), 0.03, 0.03, 3_000),
+    "wide_cells": ((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 0.1, 0.045, 60_000),
+}
+
+
+@pytest.mark.parametrize("kernel", [0, 1, 6, 10, 11])
+@pytest.mark.parametrize("geom", list(GEOMETRIES))
+def test_config_forces_geometries(torch_cuda, ctx, geom, kernel):
+    import ljcell
+
+    torch = torch_cuda
+    lo, hi, width, rc, n = GEOMETRIES[geom]
+    rng = np.random.default_rng(len(geom) * 31 + n)
+    lo32, hi32 = np.array(lo, np.float32), np.array(hi, np.float32)
+    pts = (lo32 + (hi32 - lo32) * rng.random((n, 3), dtype=np.float32)).astype(np.float32)
+    x, y, z = (np.ascontiguousarray(pts[:, k]) for k in range(3))
+    g = ljcell.grid_from_box(lo, hi, width)
+    og = O.grid_from_box(lo, hi, width)
+    assert tuple(og.dim) == tuple(g.dim)
+    p = ljcell.params(rc)
+    ctx.set_tuning(kernel)
+    try:
+        b = ctx.bin(g, dev(torch, x), dev(torch, y), dev(torch, z), order=1)
+        energy, force, tot = ctx.compute(g, p, b)
+        ctx.sync()
+    finally:
+        ctx.set_tuning(0)
+    ob = O.bin_particles(og, x, y, z, O.ORDER_X)
+    assert np.array_equal(np_(b.offsets), ob.offsets)
+    ref = O.config_forces(og, ob, rc, 1.0, p.sigma)
+    t = ljcell.totals_from_tensor(tot)
+    assert t["pairs"] == ref.pairs and ref.pairs > 0
+    fe = ref.force_errors(np_(force)[:n], FORCE_SCALED_TOL)
+    ee = ref.energy_errors(np_(energy)[:n], ENERGY_SCALED_TOL)
+    assert fe["max_scaled_over_tol"] <= 1.0 and fe["normwise"] <= FORCE_NORMWISE_TOL, fe
+    assert ee["max_scaled_over_tol"] <= 1.0, ee
