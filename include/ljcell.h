@@ -48,7 +48,11 @@ typedef enum {
     LJ_ECUDA = 3,        /* a CUDA runtime call failed */
     LJ_ETIMEOUT = 4,     /* a bounded device-side wait gave up */
     LJ_ERANGE = 5,       /* non-finite particle coordinate seen by the binning */
-    LJ_EUNSUPPORTED = 6  /* size or mode outside what this build supports */
+    LJ_EUNSUPPORTED = 6, /* size or mode outside what this build supports */
+    LJ_ECHECK = 7        /* a consistency check of the bounds-checked build (libljcell_checks.so,
+                            compiled with -DLJ_CHECKS) failed: negative count, offsets that do not
+                            match the counts, a ticket outside its cell, a sorted record outside its
+                            cell's range, out of order, or a permutation that is not a bijection */
 } lj_status;
 
 /* Within-cell order of the sorted particles.  The reference's order comes

@@ -62,6 +62,7 @@ extern "C" const char* lj_status_str(lj_status s) {
         case LJ_ETIMEOUT: return "bounded device wait timed out";
         case LJ_ERANGE: return "non-finite coordinate or out-of-range index";
         case LJ_EUNSUPPORTED: return "unsupported size or mode";
+        case LJ_ECHECK: return "consistency check failed (-DLJ_CHECKS build)";
     }
     return "unknown status";
 }
@@ -112,6 +113,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->step);
     cudaFree(c->half);
     cudaFree(c->sel);
+    cudaFree(c->check);
     if (c->e2ea_ready) {
         cudaStreamSynchronize(c->up_stream);
         for (int i = 0; i < kE2EASlots + 7; ++i) cudaEventDestroy(c->e2ea_ev[i]);
@@ -159,6 +161,7 @@ extern "C" lj_status lj_sync(lj_ctx* c) {
     if (flags) {
         if (cudaMemset(c->d_status, 0, sizeof(unsigned)) != cudaSuccess) return LJ_ECUDA;
         if (flags & kFlagTimeout) return LJ_ETIMEOUT;
+        if (flags & kFlagCheck) return LJ_ECHECK;
         return LJ_ERANGE;
     }
     return LJ_OK;

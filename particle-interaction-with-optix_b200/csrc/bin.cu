@@ -460,6 +460,63 @@ __global__ void __launch_bounds__(256) k_candidates(GridDev g, const int* __rest
     }
 }
 
+#ifdef LJ_CHECKS
+// ---------------------------------------------------------------- consistency checks (-DLJ_CHECKS)
+// The bounds-checked build (libljcell_checks.so) verifies after each binning stage what the next
+// stage relies on; a violation ORs kFlagCheck into the status word, which lj_sync reports as
+// LJ_ECHECK.  The checks only read their buffers (and mark one scratch array); none traps.
+
+// Counts are non-negative and offsets[c + 1] - offsets[c] = counts[c], offsets[0] = 0.
+__global__ void k_chk_scan(const int* __restrict__ counts, const int* __restrict__ offsets, long long nc,
+                           unsigned* status) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < nc;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int k = counts[c], a = offsets[c], b = offsets[c + 1];
+        if (k < 0 || b - a != k || (c == 0 && a != 0)) atomicOr(status, kFlagCheck);
+    }
+}
+
+// Each particle's (cell, ticket): a cell of the grid, a ticket below that cell's count.
+__global__ void k_chk_tickets(const int2* __restrict__ ct, const int* __restrict__ counts, int n, long long nc,
+                              unsigned* status) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int2 v = ct[i];
+        if (v.x < 0 || v.x >= nc || v.y < 0 || v.y >= counts[v.x]) atomicOr(status, kFlagCheck);
+    }
+}
+
+// Sorted records: original index in [0, n) (marked in seen), cell in [0, nc) with the record inside
+// the cell's offset range, cells non-decreasing, the within-cell order strict, and (single system)
+// the cell recomputed from the stored position equal to the stored one.
+template <int ORDER>
+__global__ void k_chk_sorted(GridDev g, int recompute, const float4* __restrict__ xyzi, const int* __restrict__ cell,
+                             const int* __restrict__ offsets, int n, long long nc, int* __restrict__ seen,
+                             unsigned* status) {
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+        const float4 r = xyzi[s];
+        const int i = __float_as_int(r.w), c = cell[s];
+        bool bad = i < 0 || i >= n || c < 0 || c >= nc;
+        if (!bad) {
+            atomicAdd(&seen[i], 1);
+            bad = s < offsets[c] || s >= offsets[c + 1];
+        }
+        if (!bad && recompute && isfinite(r.x) && isfinite(r.y) && isfinite(r.z)) bad = cell_of(g, r.x, r.y, r.z) != c;
+        if (!bad && s > 0) {
+            const float4 q = xyzi[s - 1];
+            const int cp = cell[s - 1];
+            bad = cp > c || (cp == c && key_less<ORDER>(r.x, i, q.x, __float_as_int(q.w)));
+        }
+        if (bad) atomicOr(status, kFlagCheck);
+    }
+}
+
+// Every original index seen exactly once: the sorted order is a permutation.
+__global__ void k_chk_seen(const int* __restrict__ seen, int n, unsigned* status) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (seen[i] != 1) atomicOr(status, kFlagCheck);
+}
+#endif
+
 // ---------------------------------------------------------------- host side
 
 static lj_status check_grid(const lj_grid* g, long long* ncells) {
@@ -485,6 +542,10 @@ lj_status launch_scan(lj_ctx* ctx, const int* counts, long long ncells, int* off
     const int vec_ok = ((reinterpret_cast<uintptr_t>(counts) | reinterpret_cast<uintptr_t>(offsets)) & 15) == 0;
     k_scan<<<(unsigned)ntiles, kScanThreads, 0, ctx->stream>>>(counts, offsets, ncells, ntiles, states, counter,
                                                               vec_ok, ctx->d_status);
+#ifdef LJ_CHECKS
+    if ((s = last_launch_status()) != LJ_OK) return s;
+    k_chk_scan<<<grid_for(ctx, ncells, 256), 256, 0, ctx->stream>>>(counts, offsets, ncells, ctx->d_status);
+#endif
     return last_launch_status();
 }
 
@@ -558,6 +619,12 @@ lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const flo
     lj_status s;
     cudaStream_t st = ctx->stream;
     if ((s = launch_scan(ctx, counts, nc, offsets)) != LJ_OK) return s;
+#ifdef LJ_CHECKS
+    if (n > 0) {
+        k_chk_tickets<<<grid_for(ctx, n, 256), 256, 0, st>>>(ctx->cell_ticket, counts, n, nc, ctx->d_status);
+        if ((s = last_launch_status()) != LJ_OK) return s;
+    }
+#endif
     if (n > 0) {
         // passes: the tuning's scatter_passes, else enough that each pass writes about kScatterRegion bytes
         long long passes = ctx->tuning.scatter_passes;
@@ -598,6 +665,25 @@ lj_status bin_finish(lj_ctx* ctx, long long nc, int n, const float* x, const flo
     if (cells) {
         k_descriptors<<<grid_for(ctx, nc, 256), 256, 0, st>>>(offsets, nc, cells);
     }
+#ifdef LJ_CHECKS
+    // the permutation check needs scratch, which cannot be allocated while a graph is being captured
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &capturing) != cudaSuccess) return LJ_ECUDA;
+    if (n > 0 && capturing == cudaStreamCaptureStatusNone) {
+        if ((s = grow(&ctx->check, &ctx->check_bytes, (size_t)n * sizeof(int))) != LJ_OK) return s;
+        int* seen = static_cast<int*>(ctx->check);
+        if (cudaMemsetAsync(seen, 0, (size_t)n * sizeof(int), st) != cudaSuccess) return LJ_ECUDA;
+        const float4* x4 = reinterpret_cast<const float4*>(sorted_xyzi);
+        if (order == LJ_ORDER_X)
+            k_chk_sorted<LJ_ORDER_X><<<grid_for(ctx, n, 256), 256, 0, st>>>(g, sys == nullptr, x4, sorted_cell, offsets,
+                                                                            n, nc, seen, ctx->d_status);
+        else
+            k_chk_sorted<LJ_ORDER_INDEX><<<grid_for(ctx, n, 256), 256, 0, st>>>(g, sys == nullptr, x4, sorted_cell,
+                                                                                offsets, n, nc, seen, ctx->d_status);
+        if ((s = last_launch_status()) != LJ_OK) return s;
+        k_chk_seen<<<grid_for(ctx, n, 256), 256, 0, st>>>(seen, n, ctx->d_status);
+    }
+#endif
     return last_launch_status();
 }
 

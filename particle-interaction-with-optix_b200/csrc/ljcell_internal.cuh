@@ -23,6 +23,7 @@ enum : unsigned {
     kFlagNonFinite = 1u << 0,  // a coordinate was NaN or Inf
     kFlagTimeout = 1u << 1,    // a bounded spin-wait gave up
     kFlagRange = 1u << 2,      // an index fell outside its buffer (defensive check)
+    kFlagCheck = 1u << 3,      // a consistency check of the -DLJ_CHECKS build failed
 };
 
 // Grid passed by value to kernels.
@@ -127,6 +128,8 @@ struct lj_ctx {
     size_t half_bytes;
     void* sel;                   // lj_select_layers: per-block counts, then offsets
     size_t sel_bytes;
+    void* check;                 // -DLJ_CHECKS build: per-particle marks of the permutation check
+    size_t check_bytes;
     // end-to-end buffers (lj_simulate_host): device buffers, a second stream for the device-to-host
     // copies and the events that order it after the pair chunks
     void* e2e;

@@ -17,9 +17,10 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libljcell.so")
+# LJCELL_CHECKS=1 loads the bounds-checked debug build (compiled with -DLJ_CHECKS) instead
+LIB_PATH = os.path.join(_HERE, "libljcell_checks.so" if os.environ.get("LJCELL_CHECKS") == "1" else "libljcell.so")
 
-LJ_OK, LJ_EINVAL, LJ_ENOMEM, LJ_ECUDA, LJ_ETIMEOUT, LJ_ERANGE, LJ_EUNSUPPORTED = range(7)
+LJ_OK, LJ_EINVAL, LJ_ENOMEM, LJ_ECUDA, LJ_ETIMEOUT, LJ_ERANGE, LJ_EUNSUPPORTED, LJ_ECHECK = range(8)
 ORDER_INDEX = 0
 ORDER_X = 1
 

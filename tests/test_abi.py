@@ -37,12 +37,24 @@ def test_library_exports_every_declared_symbol():
     assert set(ljcell.ABI_SYMBOLS) == set(declared_symbols())
 
 
+def test_checked_build_exports_the_same_symbols():
+    """The bounds-checked debug build (-DLJ_CHECKS, libljcell_checks.so) is the same ABI."""
+    import ljcell
+
+    path = os.path.join(os.path.dirname(ljcell.LIB_PATH), "libljcell_checks.so")
+    assert os.path.exists(path), "make builds libljcell_checks.so beside libljcell.so"
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\sT\s(lj_\w+)$", out, flags=re.M))
+    assert set(declared_symbols()) <= exported
+
+
 def test_abi_version_and_status_strings():
     import ljcell
 
     assert ljcell.lib().lj_abi_version() == 1
     assert ljcell.status_str(ljcell.LJ_OK) == "ok"
     assert "timed out" in ljcell.status_str(ljcell.LJ_ETIMEOUT)
+    assert "LJ_CHECKS" in ljcell.status_str(ljcell.LJ_ECHECK)
 
 
 def test_grid_from_box_matches_oracle():
