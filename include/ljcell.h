@@ -380,6 +380,11 @@ LJ_API lj_status lj_test_scan_withheld_tile(lj_ctx* ctx, const int* counts, long
 /* The same failure path for lj_exclusive_scan_noalloc, on its fixed array: every bounded look-back
  * wait gives up and the call marks its result invalid with offsets[ncells] = -1.  ncells > 8192. */
 LJ_API lj_status lj_test_scan_noalloc_withheld_tile(const int* counts, long long ncells, int* offsets, void* stream);
+/* Allocation-failure injection (no counterpart in the reference): the k-th next
+ * growth of a context's scratch memory, in any context of the process, fails
+ * as a cudaMalloc failure would (the call returns LJ_ENOMEM, the context stays
+ * usable); k = 0 turns the hook off.  For tests; not for concurrent use. */
+LJ_API lj_status lj_test_fail_alloc(int k);
 
 /* ------------------------------------------------------------- time step
  * One velocity-Verlet step of the truncated law with rebinning (no stage of

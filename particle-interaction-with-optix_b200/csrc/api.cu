@@ -1,4 +1,5 @@
 // api.cu -- context, scratch memory, status and the end-to-end entry of the C ABI.
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -8,6 +9,13 @@
 
 namespace ljc {
 
+namespace {
+// Test hook (lj_test_fail_alloc): the number of scratch growths until one is made to fail; 0 = off.
+std::atomic<int> g_fail_alloc{0};
+}  // namespace
+
+// Grows a scratch buffer to at least `need` bytes.  On failure *p is null and *cap 0 (the old
+// buffer is already freed), so the caller's next call grows it again.
 lj_status grow(void** p, size_t* cap, size_t need) {
     if (need <= *cap && *p) return LJ_OK;
     if (*p) {
@@ -15,6 +23,10 @@ lj_status grow(void** p, size_t* cap, size_t need) {
         *p = nullptr;
         *cap = 0;
     }
+    int left = g_fail_alloc.load();
+    while (left > 0 && !g_fail_alloc.compare_exchange_weak(left, left - 1)) {
+    }
+    if (left == 1) return LJ_ENOMEM;  // the growth the test hook selected
     size_t want = need + need / 8 + 256;
     if (cudaMalloc(p, want) != cudaSuccess) {
         cudaGetLastError();
@@ -52,6 +64,12 @@ struct DeviceScope {
 using namespace ljc;
 
 extern "C" int lj_abi_version(void) { return LJCELL_ABI_VERSION; }
+
+extern "C" lj_status lj_test_fail_alloc(int k) {
+    if (k < 0) return LJ_EINVAL;
+    g_fail_alloc.store(k);
+    return LJ_OK;
+}
 
 extern "C" const char* lj_status_str(lj_status s) {
     switch (s) {

@@ -591,19 +591,28 @@ lj_status bin_prepare(lj_ctx* ctx, int n, long long nc, int* counts) {
         void* p1 = ctx->cell_ticket;
         void* p2 = ctx->tmp4;
         size_t c1 = ctx->part_cap * sizeof(int2), c2 = ctx->part_cap * sizeof(float4);
-        if ((s = grow(&p1, &c1, need * sizeof(int2))) != LJ_OK) return s;
+        // a failed growth has freed its old buffer: record the null pointer and a zero capacity
+        // so that no freed buffer is used or freed again
+        s = grow(&p1, &c1, need * sizeof(int2));
         ctx->cell_ticket = static_cast<int2*>(p1);
-        if ((s = grow(&p2, &c2, need * sizeof(float4))) != LJ_OK) return s;
-        ctx->tmp4 = static_cast<float4*>(p2);
+        if (s == LJ_OK) {
+            s = grow(&p2, &c2, need * sizeof(float4));
+            ctx->tmp4 = static_cast<float4*>(p2);
+        }
+        if (s != LJ_OK) {
+            ctx->part_cap = 0;
+            return s;
+        }
         ctx->part_cap = need;
     }
     const size_t large_need = (size_t)std::max<long long>(kLargeCapMin, (long long)n / kRankMax + 1);
     if (!ctx->large_cells || ctx->large_cap < large_need) {
         void* p = ctx->large_cells;
         size_t cap = ctx->large_cells ? sizeof(int) * (1 + ctx->large_cap) : 0;
-        if ((s = grow(&p, &cap, sizeof(int) * (1 + large_need))) != LJ_OK) return s;
+        s = grow(&p, &cap, sizeof(int) * (1 + large_need));
         ctx->large_cells = static_cast<int*>(p);
-        ctx->large_cap = large_need;
+        ctx->large_cap = s == LJ_OK ? large_need : 0;
+        if (s != LJ_OK) return s;
     }
     if (cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, ctx->stream) != cudaSuccess) return LJ_ECUDA;
     if (cudaMemsetAsync(ctx->large_cells, 0, sizeof(int), ctx->stream) != cudaSuccess) return LJ_ECUDA;

@@ -138,6 +138,7 @@ def _load() -> C.CDLL:
                                    C.POINTER(Totals)]),
         "lj_simulate_host_wait": (i32, [vp]),
         "lj_select_layers": (i32, [vp, C.POINTER(Grid), i32, vp, i32, i32, vp, vp, vp]),
+        "lj_test_fail_alloc": (i32, [i32]),
         "lj_simulate_host_inorder_async": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp,
                                            C.POINTER(Totals)]),
         "lj_simulate_host_inorder": (i32, [vp, C.POINTER(Grid), C.POINTER(Params), i32, vp, vp, vp, vp, vp,
@@ -159,7 +160,7 @@ ABI_SYMBOLS = ("lj_abi_version", "lj_status_str", "lj_create", "lj_destroy", "lj
                "lj_batch_run_separate", "lj_batch_autotune", "lj_pack_mixed", "lj_compute_mixed",
                "lj_test_scan_withheld_tile", "lj_test_scan_noalloc_withheld_tile", "lj_compute_half", "lj_compute_range", "lj_reorder", "lj_step_verlet", "lj_simulate_host",
                "lj_simulate_host_async", "lj_simulate_host_wait", "lj_simulate_host_inorder_async",
-               "lj_simulate_host_inorder", "lj_select_layers")
+               "lj_simulate_host_inorder", "lj_select_layers", "lj_test_fail_alloc")
 
 
 def lib() -> C.CDLL:
@@ -194,6 +195,11 @@ def grid_compat(box_width: float, cutoff: float) -> Grid:
 def default_sigma(cutoff: float) -> float:
     """sigma = r_c / 2.5 evaluated in float32."""
     return float(np.float32(cutoff) / np.float32(2.5))
+
+
+def test_fail_alloc(k: int):
+    """lj_test_fail_alloc: make the k-th next scratch growth fail with LJ_ENOMEM (0: off)."""
+    _check(_lib.lj_test_fail_alloc(int(k)), "lj_test_fail_alloc")
 
 
 def exclusive_scan_noalloc(counts, offsets, stream=None):
