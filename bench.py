@@ -53,8 +53,6 @@ RETIRED = {2: 1, 3: 1, 4: 1, 5: 6, 7: 6, 8: 10, 9: 10}   # tuning values of reti
 
 def kernel_name(k: int) -> str:
     return KERNEL_NAMES[RETIRED.get(k, k)]
-# launches of the pair stage per lj_compute call (one for every kernel)
-PAIR_LAUNCHES = {}
 SCATTER_REGION = 56 << 20   # bytes of scattered records per binning scatter pass (the library's default)
 
 
@@ -87,7 +85,31 @@ def parse():
                     help="run the headline with this lj_tuning.pair_kernel instead of the autotuner's choice (profiling)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other workloads (batched 512 systems, sphere shell, dense) reported beside the headline")
+    ap.add_argument("--n", type=int, default=None, help="particles per GPU (overrides the --config preset)")
+    ap.add_argument("--rc", type=float, default=None, help="cutoff = cell width (overrides the --config preset)")
+    ap.add_argument("--dist", default=None, choices=["uniform", "shell"],
+                    help="uniform in [0,1)^3, or a unit sphere shell in [-0.5,1.5)^3 (overrides the preset)")
+    ap.add_argument("--mode", default="config", choices=["config", "compat", "mixed"],
+                    help="config: truncated law with forces (the benchmark); compat: the reference's law over the "
+                         "27 cells (value counts candidate pairs); mixed: binary16 cell-relative records")
     return ap.parse_args()
+
+
+def workload(args) -> dict:
+    """The --config preset with the --n / --rc / --dist overrides applied."""
+    cfg = dict(CONFIGS[args.config])
+    if args.dist == "uniform":
+        cfg.update(dist="uniform", lo=(0, 0, 0), hi=(1, 1, 1))
+    elif args.dist == "shell":
+        cfg.update(dist="sphere", lo=(-0.5,) * 3, hi=(1.5,) * 3)
+    if args.n is not None:
+        cfg["n"] = args.n
+    if args.rc is not None:
+        cfg["rc"] = args.rc
+    if args.n is not None or args.rc is not None or args.dist is not None:
+        kind = "uniform" if cfg["dist"] == "uniform" else "sphere-shell"
+        cfg["workload"] = f"{kind} {cfg['n']}, rc={cfg['rc']}"
+    return cfg
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -286,19 +308,37 @@ def run_ours(args, cfg):
     else:
         soa, _ = ctx.generate_sphere(seed, n, (0.5, 0.5, 0.5), 1.0)
     x, y, z = soa["x"], soa["y"], soa["z"]
-    b = ctx.alloc_binned(g, n, ljcell.ORDER_X)
+    mode = args.mode
+    order = ljcell.ORDER_INDEX if mode == "compat" else ljcell.ORDER_X
+    b = ctx.alloc_binned(g, n, order)
     energy, force, tot = ctx.alloc_outputs(n)
+    rec = ctx.pack_mixed(g, ctx.bin(g, x, y, z, order=order, out=b)) if mode == "mixed" else None
     cand = torch.zeros(1, dtype=torch.int64, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
+    def bin_stage():
+        ctx.bin(g, x, y, z, order=order, out=b)
+
+    def pair_stage():
+        if mode == "config":
+            ctx.compute(g, p, b, energy, force, tot)
+        elif mode == "mixed":        # records packed in every step, counted in the pair stage
+            ctx.pack_mixed(g, b, rec)
+            ctx.compute_mixed(g, p, b, rec, energy, force, tot)
+        else:                        # the reference's law (energies only, every particle of the 27 cells)
+            ctx.compute_compat(g, b, energy)
+
     def step():
-        ctx.bin(g, x, y, z, order=ljcell.ORDER_X, out=b)
-        ctx.compute(g, p, b, energy, force, tot)
+        bin_stage()
+        pair_stage()
 
     for _ in range(max(args.warmup, 3)):
         step()
     ctx.sync()
-    if args.pair_kernel:
+    if mode != "config":
+        pair_kernel = args.pair_kernel
+        ctx.set_tuning(pair_kernel)
+    elif args.pair_kernel:
         pair_kernel = args.pair_kernel
         ctx.set_tuning(pair_kernel)
     else:
@@ -308,7 +348,8 @@ def run_ours(args, cfg):
     ctx.count_candidates(g, b.offsets, cand)
     ctx.sync()
     c_ref = int(cand.item())
-    pairs = ljcell.totals_from_tensor(tot)["pairs"]
+    # compat: every candidate is an interaction of the reference's law (no cutoff)
+    pairs = c_ref if mode == "compat" else ljcell.totals_from_tensor(tot)["pairs"]
 
     K = args.steps
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
@@ -319,9 +360,9 @@ def run_ours(args, cfg):
         for k in range(K):
             flush.fill_(k & 0xFF)                      # L2 flush, outside the timed events
             ev[k][0].record(stream)
-            ctx.bin(g, x, y, z, order=ljcell.ORDER_X, out=b)
+            bin_stage()
             ev[k][1].record(stream)
-            ctx.compute(g, p, b, energy, force, tot)
+            pair_stage()
             ev[k][2].record(stream)
         torch.cuda.synchronize()
     if ws > 1:
@@ -338,16 +379,18 @@ def run_ours(args, cfg):
     sm_mhz = clocks["sm_mhz"] or 1965.0
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     peak_tflops = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
-    algo_flops = FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs
+    # compat: the reference's own count, 18 flop per candidate (cudaLJ.cu:550)
+    algo_flops = 18 * c_ref if mode == "compat" else FLOP_CANDIDATE * c_ref + FLOP_INTERACTING * pairs
     pair_ms = float(np.median(t_pair))
     achieved = algo_flops / (pair_ms * 1e-3) / 1e12
-    useful = FLOP_INTERACTING * pairs / (pair_ms * 1e-3) / 1e12
-    kname = kernel_name(pair_kernel)
+    useful = (algo_flops if mode == "compat" else FLOP_INTERACTING * pairs) / (pair_ms * 1e-3) / 1e12
+    kname = {"config": kernel_name(pair_kernel) if pair_kernel else "", "mixed": "k_pair_mixed_pass2",
+             "compat": "k_pair_compat"}[mode]
     traffic = read_traffic(kname, cfg["workload"])
 
     # errors of the last step's outputs against an FP64 reference on a stratified target sample
     errors = None
-    if rank == 0:
+    if rank == 0 and mode != "compat":
         smp = fp64_sample(g, b.offsets, b.cell[:n], b.xyzi[:n, :3].double(), rc, p.sigma)
         errors = error_stats(*smp, energy[:n], force[:n])
         errors["reference"] = "FP64 (torch, on the GPU) on the same positions, every particle of the 27-cell stencil"
@@ -355,7 +398,7 @@ def run_ours(args, cfg):
 
     # the reference law on the same particles (our compat kernel), comparable with the reference arm's pair kernel
     compat = None
-    if rank == 0 and ws == 1 and cfg["dist"] == "uniform":
+    if rank == 0 and ws == 1 and cfg["dist"] == "uniform" and mode == "config":
         gc = ljcell.grid_compat(float(cfg["hi"][0]), rc) if tuple(cfg["lo"]) == (0, 0, 0) else g
         bc = ctx.bin(gc, x, y, z, order=ljcell.ORDER_INDEX)
         vc = ctx.compute_compat(gc, bc)
@@ -374,12 +417,12 @@ def run_ours(args, cfg):
         del bc, vc, cc
 
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and mode == "config":   # the host-buffer entry computes the truncated law
         e2e = run_e2e(ctx, g, p, x, y, z, n, K, ws, dev, total_pairs, pairs)
 
 
     extras = None
-    if rank == 0 and ws == 1 and not args.no_extras:
+    if rank == 0 and ws == 1 and not args.no_extras and mode == "config":
         extras = run_extras(ctx, dev, flush, peak_tflops)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -394,9 +437,13 @@ def run_ours(args, cfg):
             "ms_per_step": t_max_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded drand48, device generated)",
             "config": {"workload": cfg["workload"], "n_per_gpu": n, "cutoff": rc, "sigma": p.sigma,
-                       "cells": g.ncells, "order": "x-sorted within cells", "mode": "plain fp32",
+                       "cells": g.ncells,
+                       "order": "x-sorted within cells" if order == ljcell.ORDER_X else "index order within cells",
+                       "mode": {"config": "plain fp32", "mixed": "mixed: binary16 cell-relative y, z records",
+                                "compat": "reference law over the 27 cells; pairs = candidate pairs"}[mode],
                        "pair_kernel": f"{pair_kernel} ({kname}, " + ("set by --pair-kernel)" if args.pair_kernel else
-                                                                     "chosen by lj_autotune_compute)"),
+                                                                     "chosen by lj_autotune_compute)")
+                       if mode == "config" else kname,
                        "l2": "flushed between steps (256 MiB write), flush excluded from timing",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single gpu"},
             "stage_ms": {"bin": float(np.median(t_bin)), "pair": pair_ms, "statistic": f"median of {K} steps",
@@ -411,7 +458,7 @@ def run_ours(args, cfg):
                                         "SM clock; MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
                          "algorithmic_flops": algo_flops},
             "e2e": e2e,
-            "gpu_launches": (bin_launches(n, g.ncells) + PAIR_LAUNCHES.get(pair_kernel, 1)) * K,
+            "gpu_launches": (bin_launches(n, g.ncells) + (2 if mode == "mixed" else 1)) * K,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         }
         if cpu:
@@ -795,7 +842,7 @@ def run_e2e(ctx, g, p, x, y, z, n, K, ws, dev, total_pairs, pairs):
     hxn, hyn, hzn, hen, hfn, hin = (t.numpy() for t in (hx, hy, hz, he, hf, hidx))
     for _ in range(2):
         ctx.simulate_host(g, p, hxn, hyn, hzn, hen, hfn, hin)
-    steps = max(3, min(K, 20))
+    steps = 30   # fixed: the pipelined steps need a run long enough that filling and draining it do not count
     if ws > 1:
         torch.distributed.barrier()
     t0 = time.perf_counter()
@@ -879,7 +926,7 @@ def reference_gpu(cfg, seed):
 
 def main():
     args = parse()
-    cfg = CONFIGS[args.config]
+    cfg = workload(args)
     if args.impl == "reference":
         return run_reference(args, cfg)
     return run_ours(args, cfg)
