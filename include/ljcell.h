@@ -232,7 +232,10 @@ LJ_API lj_status lj_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, i
  * energy and force written at those indices, totals over those targets.  The piece a
  * domain-decomposed step needs (no counterpart in the reference, which is single-GPU): a rank bins
  * its own particles and a one-cell halo received from its neighbours, and evaluates its own
- * particles, one contiguous sorted range when the domain is a range of z layers. */
+ * particles, one contiguous sorted range when the domain is a range of z layers.  Each target's
+ * results carry the bits lj_compute gives it with the same pair kernel.  With the tuning's
+ * pair_kernel 0 the kernel is chosen, as by lj_compute, from n over the whole grid's cell count;
+ * a caller whose particles fill only part of the grid sets the kernel (lj_set_tuning). */
 LJ_API lj_status lj_compute_range(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n, const float* sorted_xyzi,
                                   const int* sorted_cell, const int* offsets, lj_order order, int kb, int ke,
                                   float* energy, float* force, lj_totals* totals);
