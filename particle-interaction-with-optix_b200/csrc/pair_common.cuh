@@ -213,42 +213,53 @@ __device__ __forceinline__ void pair_target(const GridDev& g, const PairParams& 
     }
     int w = 0;
     int2 cur = s_win[0][tid];
-    const float rc2 = pp.rc2, sig2 = pp.sig2;
-    // Two candidates per iteration (the second masked off when the window has one left): half the loop
-    // overhead and two loads in flight.  Candidates are added in window order, as one at a time would.
-    auto body = [&](const float4& q, bool valid) {
-        const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        if (valid && r2 < rc2) {
-            const float ir2 = rcp_approx(r2);
-            const float s2 = sig2 * ir2;
-            const float s6 = s2 * s2 * s2;
-            const float s12 = s6 * s6;
-            ea += s12 - s6;
-            const float t = fmaf(2.0f, s12, -s6);
-            wa += t;
-            // force in units of 24 eps / sigma^2: t * s2 stays finite where t * ir2 would overflow
-            const float fs = t * s2;
-            fx = fmaf(fs, dx, fx);
-            fy = fmaf(fs, dy, fy);
-            fz = fmaf(fs, dz, fz);
-            ++np;
-        }
-    };
+    const float rc2 = pp.rc2;
+    const float2 sig2 = make_float2(pp.sig2, pp.sig2), two2 = make_float2(2.0f, 2.0f);
+    const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y), npz = make_float2(-pi.z, -pi.z);
+    float2 S12 = make_float2(0.f, 0.f), S6 = S12, FX = S12, FY = S12, FZ = S12;
+    // two candidates per iteration, evaluated together in the paired FP32 instructions without a
+    // branch (a miss contributes exact zeros)
     while (true) {
+        bool done = false;
         while (cur.x >= cur.y) {
-            if (++w >= nw) return;
+            if (++w >= nw) {
+                done = true;
+                break;
+            }
             cur = s_win[w][tid];
         }
+        if (done) break;
         const int j0 = cur.x;
         const bool two = j0 + 1 < cur.y;
         const int j1 = two ? j0 + 1 : j0;
         cur.x = j1 + 1;
         const float4 q0 = __ldg(&p[j0]);
         const float4 q1 = __ldg(&p[j1]);
-        body(q0, true);
-        body(q1, two);
+        const float2 dx = __fadd2_rn(make_float2(q0.x, q1.x), npx);
+        const float2 dy = __fadd2_rn(make_float2(q0.y, q1.y), npy);
+        const float2 dz = __fadd2_rn(make_float2(q0.z, q1.z), npz);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const bool in0 = r2.x < rc2, in1 = two && r2.y < rc2;
+        const float2 ir2 = make_float2(rcp_hit(in0, r2.x), rcp_hit(in1, r2.y));
+        const float2 s2 = __fmul2_rn(sig2, ir2);
+        const float2 s4 = __fmul2_rn(s2, s2);
+        const float2 s6 = __fmul2_rn(s4, s2);
+        const float2 s12 = __fmul2_rn(s6, s6);
+        S12 = __fadd2_rn(S12, s12);
+        S6 = __fadd2_rn(S6, s6);
+        const float2 t = __ffma2_rn(two2, s12, make_float2(-s6.x, -s6.y));
+        const float2 fs = __fmul2_rn(t, s2);
+        FX = __ffma2_rn(fs, dx, FX);
+        FY = __ffma2_rn(fs, dy, FY);
+        FZ = __ffma2_rn(fs, dz, FZ);
+        np += (unsigned)in0 + (unsigned)in1;
     }
+    const float s12t = S12.x + S12.y, s6t = S6.x + S6.y;
+    ea += s12t - s6t;
+    wa += fmaf(2.0f, s12t, -s6t);
+    fx += FX.x + FX.y;
+    fy += FY.x + FY.y;
+    fz += FZ.x + FZ.y;
 }
 
 float grid_slack(const lj_grid& g);
