@@ -812,8 +812,48 @@ def slab_workload(ctx, cfg, seed, flush, worlds=(2, 4, 8), reps=5):
     return out
 
 
+def verlet_workload(ctx, flush, side=215, reps=10, seed=5):
+    """Time stepping (lj_step_verlet: half kick and drift in the sorted order, rebinning from the
+    previous order, the pair stage, closing half kick) on a jittered cubic lattice of side^3 particles
+    (about 10M) with sigma = spacing / 1.12 and r_c = 2.5 sigma, dt = 2e-4: device time per step
+    beside a step that bins the same particles from a shuffled input order."""
+    import torch
+    import ljcell
+
+    rng = np.random.default_rng(seed)
+    a = 1.0 / side
+    gl = (np.arange(side) + 0.5) * a
+    X, Y, Z = np.meshgrid(gl, gl, gl, indexing="ij")
+    pts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    pts += rng.uniform(-0.05 * a, 0.05 * a, pts.shape)
+    pts = pts[rng.permutation(len(pts))].astype(np.float32)
+    n = len(pts)
+    sigma = a / 1.12
+    rc = 2.5 * sigma
+    g = ljcell.grid_from_box((0, 0, 0), (1, 1, 1), rc)
+    p = ljcell.params(rc, sigma=sigma)
+    d = [torch.from_numpy(np.ascontiguousarray(pts[:, k])).to(ctx.device) for k in range(3)]
+    b = ctx.bin(g, *d, order=ljcell.ORDER_X)
+    e, f, tot = ctx.alloc_outputs(n)
+    t_random = time_events(lambda: (ctx.bin(g, *d, order=ljcell.ORDER_X, out=b), ctx.compute(g, p, b, e, f, tot)),
+                           reps, flush)
+    vel = torch.from_numpy((rng.standard_normal((n, 3)) * 0.5).astype(np.float32)).to(ctx.device)
+    ctx.bin(g, *d, order=ljcell.ORDER_X, out=b)
+    ctx.compute(g, p, b, e, f, tot)
+    t_step = time_events(lambda: ctx.step_verlet(g, p, b, vel, f, 2e-4, 1.0, e, tot), reps, flush)
+    ctx.sync()
+    pairs = ljcell.totals_from_tensor(tot)["pairs"]
+    out = {"workload": f"jittered lattice {n} ({side}^3), rc={rc:.5f}, sigma=spacing/1.12, dt=2e-4",
+           "ms_per_verlet_step": t_step, "pairs_per_step": pairs, "pairs_per_s": pairs / (t_step * 1e-3),
+           "ms_bin_and_compute_from_shuffled_order": t_random}
+    del d, b, e, f, tot, vel
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_extras(ctx, dev, flush, peak_tflops):
     out = {}
+    out["verlet_lattice10M"] = verlet_workload(ctx, flush)
     out["slab_c2"] = slab_workload(ctx, CONFIGS["c2"], 1234, flush)
     out["half_shell_c2"] = half_workload(ctx, CONFIGS["c2"], 1234, flush, peak_tflops)
     out["half_shell_c4"] = half_workload(ctx, CONFIGS["c4"], 1234, flush, peak_tflops)
