@@ -89,6 +89,9 @@ def parse():
     ap.add_argument("--rc", type=float, default=None, help="cutoff = cell width (overrides the --config preset)")
     ap.add_argument("--dist", default=None, choices=["uniform", "shell"],
                     help="uniform in [0,1)^3, or a unit sphere shell in [-0.5,1.5)^3 (overrides the preset)")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="under torchrun: replicas (one system per rank, weak scaling; the default) or slab (one "
+                         "system split into z slabs with a one-layer halo exchange, strong scaling)")
     ap.add_argument("--mode", default="config", choices=["config", "compat", "mixed"],
                     help="config: truncated law with forces (the benchmark); compat: the reference's law over the "
                          "27 cells (value counts candidate pairs); mixed: binary16 cell-relative records")
@@ -964,11 +967,87 @@ def reference_gpu(cfg, seed):
             "scan_ms": float(ms[1]), "candidate_pairs_per_s": r.nbinter / (float(ms[5]) * 1e-3)}
 
 
+def run_slab(args, cfg):
+    """One system split over the ranks in slabs of z layers (ljcell.slab): each rank keeps its own
+    particles, and a step is the halo exchange with its neighbours (NCCL point-to-point), the binning
+    of own + halo particles and the pair stage over its own sorted range.  Every rank generates the
+    same system (one seed) and keeps its layers.  The step time is the median over the timed steps
+    of each rank's device time, the maximum over ranks; value = the whole system's interacting pairs
+    over it (strong scaling)."""
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+    init_dist("nccl" if ws > 1 else "gloo")
+    import ljcell
+    from ljcell import slab
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    ctx = ljcell.Context(dev.index, stream)
+    n, rc = cfg["n"], cfg["rc"]
+    g = ljcell.grid_from_box(cfg["lo"], cfg["hi"], rc)
+    p = ljcell.params(rc)
+    if cfg["dist"] == "uniform":
+        soa, _ = ctx.generate_uniform(args.seed, n, cfg["lo"], cfg["hi"])
+    else:
+        soa, _ = ctx.generate_sphere(args.seed, n, (0.5, 0.5, 0.5), 1.0)
+    xyz = torch.stack([soa["x"], soa["y"], soa["z"]], 1).contiguous()
+    del soa
+    dom = slab.SlabDomain.of(g, rank, ws)
+    own = dom.own(xyz)
+    del xyz
+    torch.cuda.empty_cache()
+    if ws > 1:
+        torch.distributed.barrier()
+    res = None
+    for _ in range(max(args.warmup, 3)):
+        res = slab.step(ctx, g, p, dom, own)
+    torch.cuda.synchronize()
+    K = args.steps
+    times = []
+    with ClockSampler(dev.index) as clk:
+        for _ in range(K):
+            if ws > 1:
+                torch.distributed.barrier()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            res = slab.step(ctx, g, p, dom, own)
+            b.record(stream)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+    ctx.sync()
+    t_max = allreduce_max(float(np.median(times)), ws, dev)
+    tot = slab.allreduce_totals(res.totals) if ws > 1 else ljcell.totals_from_tensor(res.totals)
+    halo = allreduce_max(float(res.halo), ws, dev)
+    if rank == 0:
+        clocks = clk.summary()
+        line = {"metric": METRIC, "value": tot["pairs"] / (t_max * 1e-3), "unit": "pairs/s", "n_gpus": ws,
+                "steps": K, "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded drand48, device generated)",
+                "config": {"workload": cfg["workload"], "n_total": n, "cutoff": rc, "cells": g.ncells,
+                           "parallelism": f"slab x{ws} (z layers, one-layer halo, NCCL point-to-point)",
+                           "l2": "not flushed (each rank's step reads its own and halo particles)"},
+                "pairs_per_step": tot["pairs"], "energy": tot["energy"], "max_halo_particles": int(halo),
+                "e2e": None, "gpu_launches": None,
+                "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     cfg = workload(args)
     if args.impl == "reference":
         return run_reference(args, cfg)
+    if args.decomp == "slab":
+        return run_slab(args, cfg)
     return run_ours(args, cfg)
 
 
