@@ -47,7 +47,8 @@ sys.path.insert(0, os.path.join(ROOT, "particle-interaction-with-optix_b200"))
 METRIC = "LJ pairs/sec @10M particles, plain vs mixed-precision/batched at ≤1e-5 err"
 FLOP_CANDIDATE = 8
 FLOP_INTERACTING = 18
-KERNEL_NAMES = {1: "k_pair_config", 6: "k_pair_pass", 10: "k_pair_pass2", 11: "k_pair_config (whole rows)"}
+KERNEL_NAMES = {1: "k_pair_config", 6: "k_pair_pass", 10: "k_pair_pass2", 11: "k_pair_config (whole rows)",
+                12: "k_pair_cellpair"}
 RETIRED = {2: 1, 3: 1, 4: 1, 5: 6, 7: 6, 8: 10, 9: 10}   # tuning values of retired variants -> the kernel they run
 
 

@@ -272,6 +272,15 @@ LJ_API lj_status lj_compute_half(lj_ctx* ctx, const lj_grid* g, const lj_params*
  *  11 = as 1 with the 9 rows walked whole (no row culling, no x-window
  *       searches): on sparse grids such as a sphere shell, where a row holds
  *       few particles, the searches cost more than the candidates they remove.
+ *  12 = targets paired inside their cell (a pair list built on the device:
+ *       flags, their scan, the list; 12 bytes per target of scratch in the
+ *       context): both targets of a lane share one 27-cell stencil, whose
+ *       non-empty rows are walked whole, end to end, all lanes in lockstep,
+ *       each candidate loaded once for both; for sparse grids (no window
+ *       searches, no lane whose targets need two stencils; the autotuner's
+ *       pick on a sphere shell and on a uniform grid of 0.5 particles per
+ *       cell).  A target's results do not depend on its partner, so
+ *       lj_compute_range gives the bits of lj_compute.
  * The values 2-5 and 7-9 named variants that never won on any benchmark
  * workload (per-lane queues, register windows, cell-block tiles staged by TMA
  * bulk copies, scalar passes, SoA pairs); they are kept as aliases of the kernel
@@ -286,7 +295,7 @@ typedef struct {
 } lj_tuning;
 
 LJ_API lj_status lj_set_tuning(lj_ctx* ctx, const lj_tuning* t);
-/* Autotuner for one system: times the pair kernels 1, 6, 10 and 11 on
+/* Autotuner for one system: times the pair kernels 1, 6, 10, 11 and 12 on
  * these binned (LJ_ORDER_X) particles and keeps the fastest in the context's
  * tuning.  Synchronises. */
 LJ_API lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj_params* p, int n,

@@ -132,6 +132,7 @@ extern "C" lj_status lj_destroy(lj_ctx* c) {
     cudaFree(c->half);
     cudaFree(c->sel);
     cudaFree(c->check);
+    cudaFree(c->cellpair);
     if (c->e2ea_ready) {
         cudaStreamSynchronize(c->up_stream);
         for (int i = 0; i < kE2EASlots + 7; ++i) cudaEventDestroy(c->e2ea_ev[i]);
@@ -158,7 +159,7 @@ extern "C" lj_status lj_set_stream(lj_ctx* c, void* stream) {
 }
 
 extern "C" lj_status lj_set_tuning(lj_ctx* c, const lj_tuning* t) {
-    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 11 || t->scatter_passes < 0 || t->scatter_passes > 8)
+    if (!c || !t || t->pair_kernel < 0 || t->pair_kernel > 12 || t->scatter_passes < 0 || t->scatter_passes > 8)
         return LJ_EINVAL;
     c->tuning = *t;
     return LJ_OK;

@@ -130,6 +130,8 @@ struct lj_ctx {
     size_t sel_bytes;
     void* check;                 // -DLJ_CHECKS build: per-particle marks of the permutation check
     size_t check_bytes;
+    void* cellpair;              // pair kernel 12: pair-opening flags, their exclusive scan, the pair list
+    size_t cellpair_bytes;
     // end-to-end buffers (lj_simulate_host): device buffers, a second stream for the device-to-host
     // copies and the events that order it after the pair chunks
     void* e2e;

@@ -286,6 +286,7 @@ lj_status launch_pair_config(lj_ctx* ctx, const lj_grid* g, const lj_params* prm
             case 8:
             case 9:
             case 10: return launch_pair_pass(ctx, g, pp, n, xyzi, cs, off, true, energy, force, totals, kb, ke);
+            case 12: return launch_pair_cellpair(ctx, g, pp, n, xyzi, cs, off, energy, force, totals, kb, ke);
             default: break;  // 1 (and 2, 3, 4): windows in shared memory; 11: whole rows (below)
         }
     }
@@ -365,8 +366,8 @@ extern "C" lj_status lj_autotune_compute(lj_ctx* ctx, const lj_grid* g, const lj
     int best = 1;
     float bt = 3.4e38f;
     lj_status st = LJ_OK;
-    static const int kCandidates[] = {1, 6, 10, 11};
-    for (int ki = 0; ki < 4 && st == LJ_OK; ++ki) {
+    static const int kCandidates[] = {1, 6, 10, 11, 12};
+    for (int ki = 0; ki < 5 && st == LJ_OK; ++ki) {
         const int k = kCandidates[ki];
         ctx->tuning.pair_kernel = k;
         float ms = 3.4e38f;

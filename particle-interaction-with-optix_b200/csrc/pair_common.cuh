@@ -267,4 +267,10 @@ float grid_slack(const lj_grid& g);
 lj_status launch_pair_pass(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
                            const int* cs, const int* off, bool two, float* energy, float* force, lj_totals* totals,
                            int kb, int ke);
+// Kernel 12 (pair_pass.cu): targets paired inside their cell, whole rows.
+lj_status launch_pair_cellpair(lj_ctx* ctx, const lj_grid* g, const PairParams& pp, int n, const float* xyzi,
+                               const int* cs, const int* off, float* energy, float* force, lj_totals* totals,
+                               int kb, int ke);
+// Exclusive scan of counts[ncells] into offsets[0..ncells] on the context's stream (bin.cu).
+lj_status launch_scan(lj_ctx* ctx, const int* counts, long long ncells, int* offsets);
 }  // namespace ljc

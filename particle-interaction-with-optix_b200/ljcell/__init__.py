@@ -59,8 +59,9 @@ class Particles(C.Structure):
 
 class Tuning(C.Structure):
     """lj_tuning: implementation choices (pair_kernel 0 default, 1 one target per thread with windows in
-    shared memory, 6 row passes, 10 row passes with two targets per lane, 11 as 1 with whole rows; the
-    retired values 2-5 and 7-9 run the kernel of their family)."""
+    shared memory, 6 row passes, 10 row passes with two targets per lane, 11 as 1 with whole rows, 12
+    targets paired inside their cell over whole rows; the retired values 2-5 and 7-9 run the kernel of
+    their family)."""
 
     _fields_ = [("pair_kernel", C.c_int), ("scatter_passes", C.c_int), ("reserved", C.c_int * 6)]
 
@@ -278,7 +279,7 @@ class Context:
         _check(_lib.lj_set_tuning(self._h, C.byref(t)), "lj_set_tuning")
 
     def autotune_compute(self, g: Grid, p: Params, b: Binned):
-        """Times pair kernels 1, 6, 10 and 11 on these binned particles and keeps the fastest."""
+        """Times pair kernels 1, 6, 10, 11 and 12 on these binned particles and keeps the fastest."""
         k = C.c_int(0)
         ms = C.c_float(0)
         _check(_lib.lj_autotune_compute(self._h, C.byref(g), C.byref(p), b.n, _ptr(b.xyzi), _ptr(b.cell),

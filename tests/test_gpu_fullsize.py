@@ -55,10 +55,10 @@ def full(request, ctx, torch_cuda):
     energy, force, tot = ctx.compute(g, p, b)
     ctx.sync()
     n = w["n"]
-    # the sparse-grid kernel the autotuner picks on the shell (11: whole rows)
+    # the sparse-grid kernels (11: whole rows; 12: cell pairs over whole rows)
     extra = {}
     if w["kind"] == "shell":
-        for k in (11,):
+        for k in (11, 12):
             ctx.set_tuning(k)
             try:
                 ek, fk, tk = ctx.compute(g, p, b)
@@ -133,8 +133,8 @@ def test_total_energy(full):
 
 
 def test_sparse_grid_kernel_on_the_shell(full):
-    """Kernel 11 (whole rows), which the autotuner picks on the shell: pair count exact, every
-    particle within tolerance, total energy within 1e-6."""
+    """The sparse-grid kernels 11 (whole rows) and 12 (cell pairs over whole rows): pair count exact,
+    every particle within tolerance, total energy within 1e-6."""
     ref, extra = full["ref"], full["gpu"]["extra"]
     if not extra:
         pytest.skip("the sparse-grid kernel is run on the shell workload")

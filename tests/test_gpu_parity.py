@@ -241,8 +241,8 @@ def test_compat_energy(torch_cuda, ctx, name, order):
 
 
 # ------------------------------------------------------------------ config law
-# (order, pair kernel): LJ_ORDER_INDEX has one kernel; LJ_ORDER_X has kernels 1, 6 and 10 (see lj_tuning)
-VARIANTS = [(0, 0), (1, 1), (1, 6), (1, 10), (1, 11)]
+# (order, pair kernel): LJ_ORDER_INDEX has one kernel; LJ_ORDER_X has kernels 1, 6, 10, 11 and 12 (see lj_tuning)
+VARIANTS = [(0, 0), (1, 1), (1, 6), (1, 10), (1, 11), (1, 12)]
 
 
 @pytest.mark.parametrize("order,kernel", VARIANTS, ids=[f"order{o}-k{k}" for o, k in VARIANTS])
@@ -314,7 +314,7 @@ def test_config_tiny_cutoff_pair_count(torch_cuda, ctx):
     assert ljcell.totals_from_tensor(tot)["pairs"] == ref.pairs
 
 
-@pytest.mark.parametrize("kernel", [1, 6, 10, 11])
+@pytest.mark.parametrize("kernel", [1, 6, 10, 11, 12])
 def test_deterministic(torch_cuda, ctx, kernel):
     import ljcell
 
@@ -334,7 +334,8 @@ def test_deterministic(torch_cuda, ctx, kernel):
 
 
 @pytest.mark.parametrize("name,kernel", [("uniform_c1", 0), ("uniform_c1", 1), ("uniform_c1", 6),
-                                         ("uniform_c1", 10), ("uniform_c1", 11), ("tiny33", 0)])
+                                         ("uniform_c1", 10), ("uniform_c1", 11), ("uniform_c1", 12),
+                                         ("tiny33", 0), ("tiny33", 12)])
 def test_simulate_host_matches_device_path(torch_cuda, ctx, name, kernel):
     """The host entry runs the pair stage in target chunks (one chunk for small
     n); per-particle outputs equal one full-range
@@ -371,7 +372,7 @@ def test_autotune_compute_picks_a_kernel_and_keeps_results(torch_cuda, ctx):
     (x, y, z), g, og, b, ob, rc = bin_both(torch_cuda, ctx, "uniform_dense", 1)
     p = ljcell.params(rc)
     kern, ms = ctx.autotune_compute(g, p, b)
-    assert kern in (1, 6, 10, 11) and ms > 0 and ctx.get_tuning()["pair_kernel"] == kern
+    assert kern in (1, 6, 10, 11, 12) and ms > 0 and ctx.get_tuning()["pair_kernel"] == kern
     _, _, tot = ctx.compute(g, p, b)
     ctx.sync()
     ctx.set_tuning(0)
@@ -466,7 +467,7 @@ def test_simulate_host_inorder_matches_sorted_entry(torch_cuda, ctx, name):
     assert all(t.pairs == st.pairs for t in tots)
 
 
-@pytest.mark.parametrize("kernel", [1, 6, 10, 11])
+@pytest.mark.parametrize("kernel", [1, 6, 10, 11, 12])
 def test_simulate_host_inorder_every_kernel(torch_cuda, ctx, kernel):
     """Each pair kernel writes a target's results at its input index in the input-order entry: the
     sorted entry's results put back through its index, bit for bit, with the same kernel."""
@@ -501,7 +502,7 @@ GEOMETRIES = {
 }
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 6, 10, 11])
+@pytest.mark.parametrize("kernel", [0, 1, 6, 10, 11, 12])
 @pytest.mark.parametrize("geom", list(GEOMETRIES))
 def test_config_forces_geometries(torch_cuda, ctx, geom, kernel):
     import ljcell

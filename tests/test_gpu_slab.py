@@ -88,7 +88,7 @@ def check(ctx, g, p, xyz, world):
     return halo
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 6, 10])
+@pytest.mark.parametrize("kernel", [0, 1, 6, 10, 12])
 @pytest.mark.parametrize("world", [2, 3, 5])
 def test_slab_ranks_match_single_domain(torch_cuda, ctx, world, kernel):
     import ljcell
