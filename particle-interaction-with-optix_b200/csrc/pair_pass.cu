@@ -139,33 +139,6 @@ __global__ void __launch_bounds__(256) k_cellpair_list(const int* __restrict__ f
     }
 }
 
-// The lane's non-empty rows (sw[0..nw), start and end) walked end to end as one sequence of L
-// candidates, all lanes of the warp in lockstep for the warp's longest sequence, two candidates per
-// step.  One pass instead of five: on a sparse grid the rows are short and their lengths vary from
-// lane to lane, so five lockstep passes would each wait for their own longest lane.  Every candidate
-// is masked against both targets' own indices (the own row is one of the windows).
-template <int BLOCK>
-__device__ __forceinline__ void walk_flat2(const float4* __restrict__ p, int ka, int kb, int kl, bool useA, bool useB,
-                                           float2 nx, float2 ny, float2 nz, const int2 (*sw)[BLOCK], int nw, int L,
-                                           float rc2, float sig2, Pass2Acc& a) {
-    const int maxL = (int)__reduce_max_sync(0xffffffffu, (unsigned)L);
-    const float2 nsig2 = make_float2(-sig2, -sig2);
-    const int t = threadIdx.x;
-    int w = 0;
-    int2 cur = nw > 0 ? sw[0][t] : make_int2(0, 0);  // (next candidate, end of its row)
-    for (int v = 0; v < maxL; v += 2) {
-        const bool ok0 = v < L, ok1 = v + 1 < L;
-        const int j0 = cur.x++;
-        if (cur.x == cur.y && w + 1 < nw) cur = sw[++w][t];
-        const int j1 = cur.x++;
-        if (cur.x == cur.y && w + 1 < nw) cur = sw[++w][t];
-        const float4 q0 = __ldg(&p[ok0 ? j0 : kl]);
-        const float4 q1 = __ldg(&p[ok1 ? j1 : kl]);
-        eval2<true>(q0, j0, ok0, useA, useB, ka, kb, nx, ny, nz, rc2, nsig2, a);
-        eval2<true>(q1, j1, ok1, useA, useB, ka, kb, nx, ny, nz, rc2, nsig2, a);
-    }
-}
-
 // One lane per pair: list[t] = a, b = a + 1 when in a's cell.  npairs is read on the device (pos[nk],
 // at most nk); the grid covers nk lanes, the most pairs there can be.
 template <int BLOCK = kPassThreads>
