@@ -259,7 +259,7 @@ LJ_API lj_status lj_compute_half(lj_ctx* ctx, const lj_grid* g, const lj_params*
  * whose launch shape is fixed at 128 threads per particle, cudaLJ.cu:519-520).
  * Results do not depend on them except in the last bits of floating-point
  * sums.  pair_kernel, for particles binned with LJ_ORDER_X:
- *   0 = default: 10 when the grid averages 2 or more particles per cell, else 6,
+ *   0 = default: 10 when the grid averages 2 or more particles per cell, else 12,
  *   1 = one thread per target, neighbours through L1, its windows in shared
  *       memory (also the kernel of LJ_ORDER_INDEX),
  *   6 = row passes: the 9 stencil rows walked in 5 warp-synchronous passes

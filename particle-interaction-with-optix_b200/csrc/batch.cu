@@ -319,6 +319,8 @@ static lj_status build_grids(lj_batch* b) {
         d.cell_base = (int)base;
         d.first = y.first;
         d.n = y.n;
+        // the two-target walk where the single-system default takes kernel 10, else one target per
+        // lane (kernel 6's walk; the persistent tile queue has no pair list for kernel 12)
         d.walk = default_pair_kernel(y.n, g) == 10 ? 3 : 1;
         base += (long long)g.dim[0] * g.dim[1] * g.dim[2];
         if (base > 2147483646LL) return LJ_EUNSUPPORTED;

@@ -30,13 +30,14 @@ namespace ljc {
 
 constexpr double kPairCell = 2.0;    // particles per cell from which the default takes two targets per lane
 
-// Default pair kernel for LJ_ORDER_X (measured on B200, 10M particles): the packed row passes with two
-// targets per lane (kernel 10) from 2 particles per cell up (10 per cell: 2.38 ms against 2.88 ms for
-// one target per lane; 80 per cell: 11.9 ms against 12.6 ms for the SoA walk); below, one target per
-// lane (0.5 per cell: 0.45 ms against 0.48 ms), where the merged windows of two targets add more
-// candidates than the shared loads save.
+// Default pair kernel for LJ_ORDER_X (measured on B200): the packed row passes with two targets per
+// lane (kernel 10) from 2 particles per cell up (10M at 10 per cell: 2.33 ms against 2.88 ms for one
+// target per lane; 80 per cell: 11.4 ms against 12.6 ms for the SoA walk); below, the targets paired
+// inside their cell over whole rows (kernel 12: a 4M sphere shell on 64M cells 0.517 ms against 0.597
+// for kernel 11 and 0.75 for kernel 6; 0.5M uniform on 100^3 cells 0.055 ms against 0.060 for
+// kernel 6), where windows merged across cells add more candidates than the shared loads save.
 int default_pair_kernel(int n, const lj_grid& g) {
-    return (double)n / ((double)g.dim[0] * g.dim[1] * g.dim[2]) >= kPairCell ? 10 : 6;
+    return (double)n / ((double)g.dim[0] * g.dim[1] * g.dim[2]) >= kPairCell ? 10 : 12;
 }
 
 template <bool XWIN>

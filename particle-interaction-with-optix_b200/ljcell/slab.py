@@ -145,15 +145,16 @@ class SlabResult:
     halo: int            # halo particles received
 
 
-# Particles per cell from which the library's default pair kernel takes two targets per lane
-# (kernel 10) instead of one (kernel 6).  The library applies it to n / ncells of the whole grid;
-# a slab fills only its own layers, so `step` applies it to the occupancy of those.
+# Particles per cell from which the library's default pair kernel takes two consecutive targets
+# per lane with x-windows (kernel 10) instead of targets paired inside their cell over whole rows
+# (kernel 12).  The library applies it to n / ncells of the whole grid; a slab fills only its own
+# layers, so `step` applies it to the occupancy of those.
 PAIR_CELL = 2.0
 
 
 def pair_kernel_for(dom: SlabDomain, targets: int) -> int:
     cells = (dom.z1 - dom.z0) * dom.gx * dom.gy
-    return 10 if targets >= PAIR_CELL * cells else 6
+    return 10 if targets >= PAIR_CELL * cells else 12
 
 
 def step(ctx, g, p, dom: SlabDomain, own_xyz, exchange=None, order=1) -> SlabResult:
