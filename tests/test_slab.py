@@ -51,6 +51,21 @@ def test_layer_split_is_a_partition():
         SlabDomain.of(g, 2, 2)
 
 
+def test_pair_kernel_rule_follows_the_own_layers():
+    """With the default tuning a rank picks the pair kernel the library's default would pick for its
+    own layers alone: two consecutive targets per lane with x-windows (10) from 2 particles per cell,
+    else targets paired inside their cell (12)."""
+    from ljcell.slab import PAIR_CELL, pair_kernel_for
+
+    g = O.grid_from_box((0, 0, 0), (1, 1, 1), 0.05)   # 20 x 20 x 20 cells
+    d = SlabDomain.of(g, 1, 4)                         # layers [5, 10): 2000 cells
+    cells = (d.z1 - d.z0) * d.gx * d.gy
+    assert cells == 2000
+    assert pair_kernel_for(d, int(PAIR_CELL * cells)) == 10
+    assert pair_kernel_for(d, int(PAIR_CELL * cells) - 1) == 12
+    assert pair_kernel_for(d, 0) == 12
+
+
 def test_z_cells_match_the_binning():
     g = O.grid_from_box((-0.25, 0, 0.125), (1, 1, 1.3), 0.07)
     rng = np.random.default_rng(3)
