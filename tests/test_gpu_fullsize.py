@@ -55,10 +55,11 @@ def full(request, ctx, torch_cuda):
     energy, force, tot = ctx.compute(g, p, b)
     ctx.sync()
     n = w["n"]
-    # the sparse-grid kernels (11: whole rows; 12: cell pairs over whole rows)
+    # the other sparse-grid kernels (the default there is 12: cell pairs over whole rows; 11: whole
+    # rows, one target per lane; 6: row passes)
     extra = {}
     if w["kind"] == "shell":
-        for k in (11, 12):
+        for k in (11, 6):
             ctx.set_tuning(k)
             try:
                 ek, fk, tk = ctx.compute(g, p, b)
@@ -133,8 +134,8 @@ def test_total_energy(full):
 
 
 def test_sparse_grid_kernel_on_the_shell(full):
-    """The sparse-grid kernels 11 (whole rows) and 12 (cell pairs over whole rows): pair count exact,
-    every particle within tolerance, total energy within 1e-6."""
+    """Kernels 11 (whole rows) and 6 (row passes) on the shell, where the default is 12: pair count
+    exact, every particle within tolerance, total energy within 1e-6."""
     ref, extra = full["ref"], full["gpu"]["extra"]
     if not extra:
         pytest.skip("the sparse-grid kernel is run on the shell workload")
